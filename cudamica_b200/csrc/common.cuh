@@ -1,0 +1,109 @@
+// Shared definitions for the AMICA EM engine's CUDA kernels (sm_100a).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace amica {
+
+constexpr int kMaxModels = 8;     // thread-block cluster size limit (portable)
+constexpr int kMaxMix = 8;
+constexpr float kLog2e = 1.4426950408889634f;
+constexpr float kLn2 = 0.6931471805599453f;
+constexpr float kTinyAbs = 1.17549435e-38f;  // FLT_MIN: |y| == 0 guard
+
+// Error flags written by kernels (bit set in ctx->d_err).
+enum : int {
+    kErrWaitTimeout = 1,      // a bounded mbarrier / flag wait gave up
+    kErrShape = 2,            // launch received a shape it was not built for
+    kErrSingular = 4,         // zero pivot while inverting A
+};
+
+// Per-(model, mixture, channel) E-step constants, derived in FP64 from the
+// parameters once per iteration and rounded to FP32:
+//   y  = s * (W x)_i - off          (s = sqrt(beta), off = s * (mu + (W c)_i))
+//   Q  = (cl2 - |y|^rho * log2 e) * ln 2
+struct __align__(16) MixParam {
+    float s, off, cl2, rho;
+};
+
+// Per-iteration control block, device resident (FP64 where the reference
+// keeps double on the host: src/amica.cu:800-806).
+struct Ctrl {
+    double lrate, lratemax, ll, ll_prev, ltc0;
+    int64_t iter, numdec, nkeep, nrej_total, rej_passes;
+    int64_t newton, ll_decreased, no_newt, last_rejected;
+    double rej_mean, rej_std;
+};
+
+// One history record per iteration (read back by the host after a run).
+struct IterRec {
+    double ll, lrate;
+    int64_t iter, newton, ll_decreased, nkeep, nrejected, pad;
+};
+
+// Layout of one CTA's partial sums (doubles), model h of a cluster:
+//   [0] LL numerator (rank 0 only), [1] vsum, then per channel cn, s2, gsum
+//   (n each), then usum, kn, ln, mn, md, bd, rn (m*n each, mixture-major),
+//   then Psi = sum_t g x^T (n*n, column-major: Psi(i,k) at k*n + i).
+struct PartLayout {
+    int n, m;
+    __host__ __device__ int cn() const { return 2; }
+    __host__ __device__ int s2() const { return 2 + n; }
+    __host__ __device__ int gs() const { return 2 + 2 * n; }
+    __host__ __device__ int mix(int k) const { return 2 + 3 * n + k * m * n; }  // k = 0..6
+    __host__ __device__ int psi() const { return 2 + 3 * n + 7 * m * n; }
+    __host__ __device__ int stride() const { return 2 + 3 * n + 7 * m * n + n * n; }
+};
+
+// Flat statistics vector (identical to the oracle's): [0] LL numerator, then
+// per model S = 1 + 2n + n*n + 7mn doubles: vsum, cnew (n), sigma2 num (n),
+// phi (n*n), usum, kappa num, lambda num, mu num, mu den, beta den, rho num.
+struct StatLayout {
+    int n, m;
+    __host__ __device__ int S() const { return 1 + 2 * n + n * n + 7 * m * n; }
+    __host__ __device__ int base(int h) const { return 1 + h * S(); }
+    __host__ __device__ int vs() const { return 0; }
+    __host__ __device__ int cn() const { return 1; }
+    __host__ __device__ int s2() const { return 1 + n; }
+    __host__ __device__ int phi() const { return 1 + 2 * n; }
+    __host__ __device__ int mix(int k) const { return 1 + 2 * n + n * n + k * m * n; }
+};
+
+enum MixStat { kUs = 0, kKn = 1, kLn = 2, kMn = 3, kMd = 4, kBd = 5, kRn = 6 };
+
+// Everything the fused E-step kernel needs, by value.
+struct EStepArgs {
+    const float* x;          // T x ldx sphered data (channels >= n are zero)
+    const float* Wf;         // M x NP x NP, W[h][i][k] row-major, zero padded
+    const float* wc;         // M x NP, (W c)_i in FP32
+    const MixParam* mp;      // M x m x NP
+    const float* ltcrel;     // M: log gm_h + ldet_h + ldetS - (same for h = 0)
+    const uint8_t* keep;     // T (nullptr = all kept)
+    float* Lt_out;           // M x T relative Lt (nullptr = skip)
+    float* P_out;            // T relative P (nullptr = skip)
+    double* partial;         // nclusters x M x stride
+    int* err;
+    int64_t T;
+    int ldx, n, M, m;
+    int ntiles, nclusters;
+    int update_rho;
+};
+
+}  // namespace amica
+
+// ---- small PTX helpers ----------------------------------------------------
+__device__ __forceinline__ float ptx_ex2(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ptx_lg2(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ptx_rcp(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}

@@ -1,0 +1,416 @@
+// Plain FP32 form of the fused AMICA E-step (SIMT FP32 contractions).
+//
+// One thread-block cluster per sample tile stream; CTA rank h of the cluster
+// owns model h (cluster size = M).  Per tile of S samples each CTA:
+//   1. stages the x tile in shared memory and computes b = W_h x on the FP32
+//      pipe (register-blocked SIMT GEMM, W_h resident in shared memory);
+//   2. evaluates the generalized-Gaussian mixture log-densities and the
+//      log-sum-exp over mixtures per (channel, sample) -- the work of
+//      betabyxminusmu / logalogblogpfun / updateltz (src/kernels.cu:251-366);
+//   3. reduces over channels to Lt_h(t) and exchanges Lt over distributed
+//      shared memory so that every CTA forms P(t) and v_h(t) (updatell,
+//      src/kernels.cu:376-450) without touching global memory;
+//   4. accumulates the sufficient statistics of src/kernels.cu:473-827 in
+//      registers and Psi_h += g x^T (the sum behind phi = g b^T of
+//      src/amica.cu:1535-1550, with phi formed from Psi in the FP64 M-step).
+// Partial sums go to a per-CTA slot of `partial`; a separate kernel reduces
+// the slots in a fixed order, so results are deterministic.
+#include <cooperative_groups.h>
+#include <cstdio>
+
+#include "common.cuh"
+
+namespace cg = cooperative_groups;
+using namespace amica;
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kS = 64;  // samples per tile
+
+template <int NP>
+struct PlainShape {
+    static constexpr int SPLIT = kThreads / NP;     // sample groups per channel
+    static constexpr int SUB = kS / SPLIT;          // samples per thread per tile
+    static constexpr int WLD = NP + 4;              // padded row of W^T in smem
+    static constexpr int XLD = NP + 4;              // padded row of the x tile
+    // GEMM b = W x: each thread 4 channels x CT samples
+    static constexpr int NTI = NP / 4;
+    static constexpr int NTT = kThreads / NTI;
+    static constexpr int CT = kS / NTT;
+    // Psi update: each thread RI x RK block
+    static constexpr int RI = NP / 16;
+    static constexpr int RK = NP / 16;
+    static constexpr size_t smem_floats =
+        (size_t)NP * WLD + (size_t)kS * XLD + (size_t)kS * NP * 2 + 2 * kS + 2 * kS;
+};
+
+template <int NP, int MM>
+__global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
+    using Sh = PlainShape<NP>;
+    extern __shared__ __align__(16) float sm[];
+    float* Wt = sm;                                   // [NP][WLD]  Wt[k][i] = W[i][k]
+    float* xs = Wt + NP * Sh::WLD;                    // [S][XLD]
+    float* bs = xs + kS * Sh::XLD;                    // [S][NP]    (W x)_i per sample
+    float* gs = bs + kS * NP;                         // [S][NP]    g, aliased with lse
+    float* slot = gs + kS * NP;                       // [2][S]     cluster-visible L_h(t)
+    float* vS = slot + 2 * kS;                        // [S]        v_h(t) (0 if not used)
+    float* spare = vS + kS;                           // [S]
+
+    cg::cluster_group cluster = cg::this_cluster();
+    const int h = (int)cluster.block_rank();
+    const int cid = blockIdx.x / a.M;
+    const int tid = threadIdx.x;
+    const int n = a.n, M = a.M;
+    if (a.m != MM || n > NP) {
+        if (tid == 0) atomicOr(a.err, kErrShape);
+    }
+
+    // ---- resident per-CTA data: W_h^T and this thread's mixture constants
+    const float* Wh = a.Wf + (size_t)h * NP * NP;
+    for (int e = tid; e < NP * NP; e += kThreads) {
+        int i = e / NP, k = e % NP;
+        Wt[k * Sh::WLD + i] = Wh[e];
+    }
+    const int ch = tid % NP;            // density-phase channel
+    const int grp = tid / NP;           // density-phase sample group
+    const bool ch_ok = ch < n;
+    float ps[MM], po[MM], pc[MM], pr[MM];
+#pragma unroll
+    for (int j = 0; j < MM; j++) {
+        MixParam q = a.mp[((size_t)h * MM + j) * NP + ch];
+        ps[j] = q.s; po[j] = q.off; pc[j] = q.cl2; pr[j] = q.rho;
+    }
+    const float wci = a.wc[(size_t)h * NP + ch];
+    float ltc[kMaxModels];
+#pragma unroll
+    for (int q = 0; q < kMaxModels; q++) ltc[q] = (q < M) ? a.ltcrel[q] : 0.f;
+
+    // FP64 running sums for this thread's channel
+    double dUs[MM], dKn[MM], dLn[MM], dMn[MM], dMd[MM], dBd[MM], dRn[MM];
+#pragma unroll
+    for (int j = 0; j < MM; j++) dUs[j] = dKn[j] = dLn[j] = dMn[j] = dMd[j] = dBd[j] = dRn[j] = 0.0;
+    double dCn = 0.0, dS2 = 0.0, dGs = 0.0;
+    double dLL = 0.0, dVs = 0.0;   // per-sample threads (tid < S)
+    float psi[Sh::RI][Sh::RK];
+#pragma unroll
+    for (int r = 0; r < Sh::RI; r++)
+#pragma unroll
+        for (int c = 0; c < Sh::RK; c++) psi[r][c] = 0.f;
+
+    int par = 0;
+    for (int tile = cid; tile < a.ntiles; tile += a.nclusters, par ^= 1) {
+        const int64_t t0 = (int64_t)tile * kS;
+        // ---- stage the x tile (float4, coalesced; rows past T are zero)
+        for (int e = tid; e < kS * (NP / 4); e += kThreads) {
+            int t = e / (NP / 4), k4 = e % (NP / 4);
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (t0 + t < a.T) v = reinterpret_cast<const float4*>(a.x + (t0 + t) * a.ldx)[k4];
+            *reinterpret_cast<float4*>(xs + t * Sh::XLD + 4 * k4) = v;
+        }
+        __syncthreads();
+        // ---- b = W_h x  (thread: channels 4*ti..+3, samples tt*CT..+CT-1)
+        {
+            const int ti = tid % Sh::NTI, tt = tid / Sh::NTI;
+            float acc[Sh::CT][4];
+#pragma unroll
+            for (int c = 0; c < Sh::CT; c++)
+#pragma unroll
+                for (int q = 0; q < 4; q++) acc[c][q] = 0.f;
+#pragma unroll 2
+            for (int k = 0; k < NP; k += 4) {
+                float4 w0 = *reinterpret_cast<const float4*>(Wt + (k + 0) * Sh::WLD + 4 * ti);
+                float4 w1 = *reinterpret_cast<const float4*>(Wt + (k + 1) * Sh::WLD + 4 * ti);
+                float4 w2 = *reinterpret_cast<const float4*>(Wt + (k + 2) * Sh::WLD + 4 * ti);
+                float4 w3 = *reinterpret_cast<const float4*>(Wt + (k + 3) * Sh::WLD + 4 * ti);
+#pragma unroll
+                for (int c = 0; c < Sh::CT; c++) {
+                    float4 xv = *reinterpret_cast<const float4*>(xs + (tt * Sh::CT + c) * Sh::XLD + k);
+                    acc[c][0] = fmaf(w0.x, xv.x, acc[c][0]); acc[c][1] = fmaf(w0.y, xv.x, acc[c][1]);
+                    acc[c][2] = fmaf(w0.z, xv.x, acc[c][2]); acc[c][3] = fmaf(w0.w, xv.x, acc[c][3]);
+                    acc[c][0] = fmaf(w1.x, xv.y, acc[c][0]); acc[c][1] = fmaf(w1.y, xv.y, acc[c][1]);
+                    acc[c][2] = fmaf(w1.z, xv.y, acc[c][2]); acc[c][3] = fmaf(w1.w, xv.y, acc[c][3]);
+                    acc[c][0] = fmaf(w2.x, xv.z, acc[c][0]); acc[c][1] = fmaf(w2.y, xv.z, acc[c][1]);
+                    acc[c][2] = fmaf(w2.z, xv.z, acc[c][2]); acc[c][3] = fmaf(w2.w, xv.z, acc[c][3]);
+                    acc[c][0] = fmaf(w3.x, xv.w, acc[c][0]); acc[c][1] = fmaf(w3.y, xv.w, acc[c][1]);
+                    acc[c][2] = fmaf(w3.z, xv.w, acc[c][2]); acc[c][3] = fmaf(w3.w, xv.w, acc[c][3]);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < Sh::CT; c++)
+                *reinterpret_cast<float4*>(bs + (tt * Sh::CT + c) * NP + 4 * ti) =
+                    make_float4(acc[c][0], acc[c][1], acc[c][2], acc[c][3]);
+        }
+        __syncthreads();
+        // ---- phase 1: per (channel, sample) log-sum-exp over mixtures (log2 units)
+        float* lse = gs;
+#pragma unroll 4
+        for (int r = 0; r < Sh::SUB; r++) {
+            const int t = grp * Sh::SUB + r;
+            const float bx = bs[t * NP + ch];
+            float q[MM], qmax = -INFINITY;
+#pragma unroll
+            for (int j = 0; j < MM; j++) {
+                float y = fmaf(ps[j], bx, -po[j]);
+                float ay = fmaxf(fabsf(y), kTinyAbs);
+                float p = ptx_ex2(pr[j] * ptx_lg2(ay));
+                q[j] = fmaf(-p, kLog2e, pc[j]);
+                qmax = fmaxf(qmax, q[j]);
+            }
+            float se = 0.f;
+#pragma unroll
+            for (int j = 0; j < MM; j++) se += ptx_ex2(q[j] - qmax);
+            lse[t * NP + ch] = ch_ok ? qmax + ptx_lg2(se) : 0.f;
+        }
+        __syncthreads();
+        // ---- Lt_h(t): channel sum in fixed order, published for the cluster
+        float* myslot = slot + par * kS;
+        if (tid < kS) {
+            float s = 0.f;
+            for (int i = 0; i < n; i++) s += lse[tid * NP + i];
+            myslot[tid] = ltc[h] + kLn2 * s;
+        }
+        cluster.sync();
+        // ---- P(t) and v_h(t) (identical arithmetic in every CTA of the cluster)
+        if (tid < kS) {
+            float L[kMaxModels];
+            float lmax = -INFINITY;
+#pragma unroll
+            for (int q = 0; q < kMaxModels; q++) {
+                if (q < M) {
+                    const float* ps_q = cluster.map_shared_rank(myslot, q);
+                    L[q] = ps_q[tid];
+                    lmax = fmaxf(lmax, L[q]);
+                }
+            }
+            float se = 0.f;
+#pragma unroll
+            for (int q = 0; q < kMaxModels; q++)
+                if (q < M) se += ptx_ex2((L[q] - lmax) * kLog2e);
+            const float P = lmax + kLn2 * ptx_lg2(se);
+            const float vh = ptx_ex2((L[h] - P) * kLog2e);
+            const int64_t tg = t0 + tid;
+            const bool valid = tg < a.T && (a.keep == nullptr || a.keep[tg]);
+            vS[tid] = valid ? vh : 0.f;
+            if (valid) {
+                dVs += (double)vh;
+                if (h == 0) dLL += (double)P;
+            }
+            if (tg < a.T) {
+                if (a.Lt_out) a.Lt_out[(size_t)h * a.T + tg] = L[h];
+                if (a.P_out && h == 0) a.P_out[tg] = P;
+            }
+        }
+        __syncthreads();
+        // ---- phase 2: responsibilities, score function and sufficient statistics
+        {
+            float fUs[MM], fKn[MM], fLn[MM], fMn[MM], fMd[MM], fBd[MM], fRn[MM];
+#pragma unroll
+            for (int j = 0; j < MM; j++) fUs[j] = fKn[j] = fLn[j] = fMn[j] = fMd[j] = fBd[j] = fRn[j] = 0.f;
+            float fCn = 0.f, fS2 = 0.f, fGs = 0.f;
+#pragma unroll 2
+            for (int r = 0; r < Sh::SUB; r++) {
+                const int t = grp * Sh::SUB + r;
+                const float v = vS[t];
+                const float bx = bs[t * NP + ch];
+                float y[MM], L2[MM], p[MM], q[MM], qmax = -INFINITY;
+#pragma unroll
+                for (int j = 0; j < MM; j++) {
+                    y[j] = fmaf(ps[j], bx, -po[j]);
+                    float ay = fmaxf(fabsf(y[j]), kTinyAbs);
+                    L2[j] = ptx_lg2(ay);
+                    p[j] = ptx_ex2(pr[j] * L2[j]);
+                    q[j] = fmaf(-p[j], kLog2e, pc[j]);
+                    qmax = fmaxf(qmax, q[j]);
+                }
+                float e[MM], se = 0.f;
+#pragma unroll
+                for (int j = 0; j < MM; j++) { e[j] = ptx_ex2(q[j] - qmax); se += e[j]; }
+                const float vr = v * ptx_rcp(se);
+                float g = 0.f;
+#pragma unroll
+                for (int j = 0; j < MM; j++) {
+                    const float u = e[j] * vr;
+                    const float ay = fmaxf(fabsf(y[j]), kTinyAbs);
+                    const float ri = ptx_rcp(ay);
+                    const float pm1 = p[j] * ri;                 // |y|^(rho-1)
+                    const float fp = copysignf(pr[j] * pm1, y[j]);
+                    const float ufp = u * fp;
+                    g = fmaf(ps[j], ufp, g);
+                    fUs[j] += u;
+                    fKn[j] = fmaf(ufp, fp, fKn[j]);
+                    const float lv = fmaf(fp, y[j], -1.f);
+                    fLn[j] = fmaf(u * lv, lv, fLn[j]);
+                    fMn[j] += ufp;
+                    if (pr[j] <= 2.f) {
+                        fMd[j] = fmaf(ufp, copysignf(ri, y[j]), fMd[j]);
+                        fBd[j] = fmaf(ufp, y[j], fBd[j]);
+                    } else {
+                        fMd[j] = fmaf(ufp, fp, fMd[j]);
+                        fBd[j] = fmaf(u, p[j], fBd[j]);
+                    }
+                    if (a.update_rho) fRn[j] = fmaf(u * p[j], pr[j] * L2[j] * kLn2, fRn[j]);
+                }
+                const float bb = bx - wci;
+                fCn = fmaf(v, xs[t * Sh::XLD + ch], fCn);
+                fS2 = fmaf(v * bb, bb, fS2);
+                fGs += g;
+                gs[t * NP + ch] = ch_ok ? g : 0.f;
+            }
+            if (ch_ok) {
+#pragma unroll
+                for (int j = 0; j < MM; j++) {
+                    dUs[j] += fUs[j]; dKn[j] += fKn[j]; dLn[j] += fLn[j]; dMn[j] += fMn[j];
+                    dMd[j] += fMd[j]; dBd[j] += fBd[j]; dRn[j] += fRn[j];
+                }
+                dCn += fCn; dS2 += fS2; dGs += fGs;
+            }
+        }
+        __syncthreads();
+        // ---- Psi_h += g x^T over the tile (thread: RI x RK block)
+        {
+            const int pi = tid % 16, pk = tid / 16;
+            const int i0 = pi * Sh::RI, k0 = pk * Sh::RK;
+#pragma unroll 4
+            for (int t = 0; t < kS; t++) {
+                float gv[Sh::RI], xv[Sh::RK];
+#pragma unroll
+                for (int r = 0; r < Sh::RI; r++) gv[r] = gs[t * NP + i0 + r];
+#pragma unroll
+                for (int c = 0; c < Sh::RK; c++) xv[c] = xs[t * Sh::XLD + k0 + c];
+#pragma unroll
+                for (int r = 0; r < Sh::RI; r++)
+#pragma unroll
+                    for (int c = 0; c < Sh::RK; c++) psi[r][c] = fmaf(gv[r], xv[c], psi[r][c]);
+            }
+        }
+        __syncthreads();
+    }
+
+    // ---- write this CTA's partial sums (fixed-order combination of groups)
+    PartLayout L{n, MM};
+    double* out = a.partial + ((size_t)cid * M + h) * L.stride();
+    double* red = reinterpret_cast<double*>(xs);   // reuse x/b/g tiles: [SPLIT][24?][NP]
+    constexpr int NACC = 7 * MM + 3;
+    {
+        double vals[NACC];
+#pragma unroll
+        for (int j = 0; j < MM; j++) {
+            vals[0 * MM + j] = dUs[j]; vals[1 * MM + j] = dKn[j]; vals[2 * MM + j] = dLn[j];
+            vals[3 * MM + j] = dMn[j]; vals[4 * MM + j] = dMd[j]; vals[5 * MM + j] = dBd[j];
+            vals[6 * MM + j] = dRn[j];
+        }
+        vals[7 * MM + 0] = dCn; vals[7 * MM + 1] = dS2; vals[7 * MM + 2] = dGs;
+#pragma unroll
+        for (int k = 0; k < NACC; k++) red[((size_t)grp * NACC + k) * NP + ch] = vals[k];
+    }
+    __syncthreads();
+    for (int e = tid; e < NACC * NP; e += kThreads) {
+        const int k = e / NP, i = e % NP;
+        if (i >= n) continue;
+        double s = 0.0;
+        for (int g2 = 0; g2 < Sh::SPLIT; g2++) s += red[((size_t)g2 * NACC + k) * NP + i];
+        if (k < 7 * MM) {
+            const int stat = k / MM, j = k % MM;
+            out[L.mix(stat) + j * n + i] = s;
+        } else if (k == 7 * MM) {
+            out[L.cn() + i] = s;
+        } else if (k == 7 * MM + 1) {
+            out[L.s2() + i] = s;
+        } else {
+            out[L.gs() + i] = s;
+        }
+    }
+    __syncthreads();
+    // LL numerator and vsum: per-sample threads, combined in fixed order
+    double* red2 = red;
+    if (tid < kS) { red2[tid] = dLL; red2[kS + tid] = dVs; }
+    __syncthreads();
+    if (tid == 0) {
+        double s0 = 0.0, s1 = 0.0;
+        for (int t = 0; t < kS; t++) { s0 += red2[t]; s1 += red2[kS + t]; }
+        out[0] = s0;
+        out[1] = s1;
+    }
+    {
+        const int pi = tid % 16, pk = tid / 16;
+        const int i0 = pi * Sh::RI, k0 = pk * Sh::RK;
+#pragma unroll
+        for (int r = 0; r < Sh::RI; r++)
+#pragma unroll
+            for (int c = 0; c < Sh::RK; c++) {
+                const int i = i0 + r, k = k0 + c;
+                if (i < n && k < n) out[L.psi() + (size_t)k * n + i] = (double)psi[r][c];
+            }
+    }
+    // peers may still read this CTA's slots: leave together
+    cluster.sync();
+}
+
+template <int NP, int MM>
+cudaError_t launch_plain(const EStepArgs& a, int nclusters, cudaStream_t st) {
+    using Sh = PlainShape<NP>;
+    const size_t smem = Sh::smem_floats * sizeof(float);
+    auto kern = estep_plain_kernel<NP, MM>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (a.M > 1) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 0);
+        if (e != cudaSuccess) return e;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nclusters * a.M);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = a.M;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, a);
+}
+
+}  // namespace
+
+namespace amica {
+
+int plain_tile_samples() { return kS; }
+
+int plain_pad_channels(int n) { return n <= 32 ? 32 : (n <= 64 ? 64 : (n <= 128 ? 128 : -1)); }
+
+// Largest cluster count whose clusters can all be resident at once.
+int plain_max_clusters(int n, int m, int M) {
+    int NP = plain_pad_channels(n);
+    if (NP < 0 || m < 1 || m > 5 || M < 1 || M > kMaxModels) return -1;
+    size_t smem = 0;
+    if (NP == 32) smem = PlainShape<32>::smem_floats * 4;
+    if (NP == 64) smem = PlainShape<64>::smem_floats * 4;
+    if (NP == 128) smem = PlainShape<128>::smem_floats * 4;
+    int dev = 0, sms = 0, maxsmem = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    int per_sm = (int)(maxsmem / (smem + 1024));
+    if (per_sm < 1) return -1;
+    int ctas = sms * per_sm;
+    return ctas / M;
+}
+
+cudaError_t launch_estep_plain(const EStepArgs& a, int NP, int nclusters, cudaStream_t st) {
+#define AMICA_PLAIN_CASE(NPV, MMV) \
+    if (NP == NPV && a.m == MMV) return launch_plain<NPV, MMV>(a, nclusters, st);
+#define AMICA_PLAIN_NP(NPV) \
+    AMICA_PLAIN_CASE(NPV, 1) AMICA_PLAIN_CASE(NPV, 2) AMICA_PLAIN_CASE(NPV, 3) \
+    AMICA_PLAIN_CASE(NPV, 4) AMICA_PLAIN_CASE(NPV, 5)
+    AMICA_PLAIN_NP(32)
+    AMICA_PLAIN_NP(64)
+    AMICA_PLAIN_NP(128)
+#undef AMICA_PLAIN_NP
+#undef AMICA_PLAIN_CASE
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace amica

@@ -1,0 +1,173 @@
+/*
+ * amica_b200.h -- C ABI of the B200-native AMICA EM engine.
+ *
+ * This is the drop-in boundary for the reference's EM loop
+ * (fraimondo/cudamica).  The reference exposes no library API: its EM loop
+ * is `error runamica(void)` (include/amica.h:123), which reads the global
+ * `currentConfig` (include/config.h:85-172) filled by `getConfig()`
+ * (src/config.c:12-213) and global device/model arrays, and exit(1)s on any
+ * failure.  Each entry point below names the piece of that loop it replaces.
+ *
+ * Conventions:
+ *   - every call returns an int status: 0 on success, the reference's codes
+ *     (include/error.h:111-118) for the same conditions, new negative codes
+ *     below for conditions the reference handles by exit(1).  Nothing calls
+ *     exit().
+ *   - caller-owned host buffers, context-owned device buffers; one context per
+ *     host thread, each on its own CUDA stream.
+ *   - layouts follow the reference's files: data T x n sample-major float32;
+ *     A and W column-major n x n per model; c n per model; alpha, mu, beta,
+ *     rho as M x m x n (channel fastest).
+ */
+#ifndef AMICA_B200_H
+#define AMICA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes: the reference's (include/error.h:111-118) ... */
+#define AMICA_OK                 0
+#define AMICA_ERR_NODEVICEMEM   (-1)
+#define AMICA_ERR_NOPARAM       (-2)
+#define AMICA_ERR_INVALIDPARAM  (-3)
+#define AMICA_ERR_INVALIDCONFIG (-4)
+#define AMICA_ERR_NOFILE        (-5)
+#define AMICA_ERR_IO            (-6)
+#define AMICA_ERR_NOMEM         (-7)
+/* ... and the engine's own */
+#define AMICA_ERR_CUDA          (-20)  /* a CUDA runtime call failed */
+#define AMICA_ERR_STATE         (-21)  /* call out of order (e.g. em_step before init) */
+#define AMICA_ERR_SINGULAR      (-22)  /* A_h not invertible */
+#define AMICA_ERR_NUMERIC       (-23)  /* NaN/Inf in LL or parameters; state rolled back */
+#define AMICA_ERR_TIMEOUT       (-24)  /* a bounded device-side wait expired */
+#define AMICA_ERR_UNSUPPORTED   (-25)  /* shape outside the compiled kernels */
+#define AMICA_ERR_NODEVICE      (-26)  /* no CUDA device / extension unusable */
+
+#define AMICA_PREC_FP32   0   /* plain FP32 form: SIMT FP32 contractions */
+#define AMICA_PREC_MIXED  1   /* tcgen05 TF32 contractions, FP32 densities */
+
+/* Replaces the reference's `config` struct (include/config.h:85-172) with the
+ * defaults of include/config.h:46-83; the rejection and precision keys are
+ * new.  All fields are 8 bytes wide. */
+typedef struct amica_cfg {
+    int64_t nchannels, nsamples, nmmodels, nsdm;
+    int64_t maxiter, do_sphere, block_size, fix_init;
+    int64_t do_newton, update_rho, rho_start_iter, newt_start_iter, maxdec;
+    int64_t update_gm, update_alpha, update_A, update_mu, update_beta, do_reparm;
+    int64_t do_reject, rejstart, rejint, maxrej;
+    int64_t precision, device, seed, verbose;
+    double lrate0, lratemax, lnatrate, lratefact, rho0, rholrate, rhomin, rhomax, rejsig;
+} amica_cfg;
+
+/* What one iteration reports; the reference prints the same quantities
+ * ("Iteration %lu: lrate %.16f LL %.16f", src/amica.cu:1983). */
+typedef struct amica_iter_out {
+    int64_t iter;          /* 1-based */
+    double  ll;            /* log-likelihood per sample and channel */
+    double  lrate;         /* learning rate in effect when LL was printed */
+    int64_t ll_decreased;  /* the "Likelihood decreasing!" branch was taken */
+    int64_t newton;        /* 1 if the A update used the Newton step */
+    int64_t nkeep;         /* samples in the sums (T minus rejected) */
+    int64_t nrejected;     /* samples dropped by this iteration's rejection pass */
+    double  device_ms;     /* device time of the iteration (CUDA events) */
+} amica_iter_out;
+
+typedef struct amica_ctx amica_ctx;
+
+/* Fill cfg with the reference's defaults (include/config.h:46-83). */
+int amica_default_cfg(amica_cfg *cfg);
+
+/* Create a context on cfg->device: replaces initializeDevs()
+ * (src/device.cu:190-380) and the allocation half of initializeModels()
+ * (src/amica.cu:135-556). */
+int amica_create(const amica_cfg *cfg, amica_ctx **out);
+
+/* Release every device and host resource: replaces finalizeModels() /
+ * finalizeDevs() (src/amica.cu:562-622, src/device.cu:382-426). */
+int amica_destroy(amica_ctx *ctx);
+
+/* Raw (unsphered) data, T x n float32 sample-major, host memory: replaces
+ * loadMatrix() + the H2D copy (src/amica.cu:671-705, src/helpers.cu:513-553). */
+int amica_load_data(amica_ctx *ctx, const float *x, int64_t n, int64_t T);
+
+/* Same, with x already in device memory (no host copy). */
+int amica_load_data_device(amica_ctx *ctx, const float *dx, int64_t n, int64_t T);
+
+/* Centring and sphering on the GPU in FP64: replaces center() and whiten()
+ * (src/preprocess.cu:31-420); do_sphere 0/1/2 as in the reference. */
+int amica_preprocess(amica_ctx *ctx);
+
+/* Use caller-provided whitened data (T x n float64), means, sphere (n x n,
+ * column-major) and ldetS instead of amica_preprocess(): the reference's
+ * deterministic mode (-DNORAND, src/amica.cu:731-734). */
+int amica_set_sphered(amica_ctx *ctx, const double *xs, const double *means,
+                      const double *sphere, double ldetS);
+
+/* Deterministic initial state: A0 (M x n x n) and c0 (M x n) as the
+ * reference's -DNORAND files give them (src/amica.cu:314-322); gm, alpha, mu,
+ * beta, rho follow fix_init (src/amica.cu:337-394).  A0 == NULL draws
+ * A = I + 0.05*(U - 0.5) with unit columns and c ~ N(0,1) from cfg->seed. */
+int amica_init(amica_ctx *ctx, const double *A0, const double *c0);
+
+/* One EM iteration: replaces one pass of the iteration body of runamica()
+ * (src/amica.cu:820-2541).  out may be NULL. */
+int amica_em_step(amica_ctx *ctx, amica_iter_out *out);
+
+/* maxiter iterations with no host synchronisation between them (one CUDA
+ * graph per iteration); hist may be NULL or hold maxiter entries. */
+int amica_run(amica_ctx *ctx, int64_t maxiter, amica_iter_out *hist);
+
+/* Current parameters (any pointer may be NULL).  W is the inverse of A used
+ * by the last E-step, as the reference's weightsfile (src/amica.cu:2546-2562). */
+int amica_get_params(amica_ctx *ctx, double *A, double *W, double *c, double *gm,
+                     double *alpha, double *mu, double *beta, double *rho);
+
+/* Overwrite the parameters (any pointer may be NULL = keep). */
+int amica_set_params(amica_ctx *ctx, const double *A, const double *c, const double *gm,
+                     const double *alpha, const double *mu, const double *beta,
+                     const double *rho);
+
+/* E-step only, at the current parameters: the FP64 sufficient statistics in
+ * the flat layout of amica_stats_len() (LL numerator, then per model vsum,
+ * cnew, sigma2 numerator, phi = sum g b^T, and the usum / kappa / lambda /
+ * mu / beta / rho sums of src/kernels.cu:495-827).  No parameter changes. */
+int amica_estep_stats(amica_ctx *ctx, double *stats);
+int64_t amica_stats_len(int64_t n, int64_t M, int64_t m);
+
+/* Per-sample outputs of the last E-step: Lt (M x T, the reference's ltall,
+ * src/amica.cu:1203-1209), P (T, per-sample log-likelihood) and the keep mask
+ * (T bytes).  Any pointer may be NULL. */
+int amica_get_loglik(amica_ctx *ctx, double *Lt, double *P, uint8_t *keep);
+
+/* Log-likelihood L (sum over kept samples of P, per sample and channel as the
+ * reference normalises it) and its gradient with respect to W (M x n x n,
+ * column-major), mu, beta and rho (M x m x n), in one sweep that recomputes
+ * the responsibilities per tile.  Any gradient pointer may be NULL. */
+int amica_loglik_adjoint(amica_ctx *ctx, double *ll, double *dW, double *dmu,
+                         double *dbeta, double *drho);
+
+/* Rejection mask of the reference-free rule (mean - rejsig*std of P over kept
+ * samples, FP64, fixed reduction order) applied to the last E-step's P. */
+int amica_reject_now(amica_ctx *ctx, int64_t *nrejected);
+
+/* Output stage: writes the reference's raw float64 files (any path may be
+ * NULL): replaces src/amica.cu:2542-2816. */
+typedef struct amica_paths {
+    const char *weightsfile, *afile, *cfile, *ltallfile, *gmfile, *alphafile,
+               *mufile, *betafile, *rhofile, *llfile, *spherefile;
+} amica_paths;
+int amica_write_outputs(amica_ctx *ctx, const amica_paths *paths);
+
+/* Message for a status code (replaces cGetErrorString, src/error.cu:14-16). */
+const char *amica_status_string(int status);
+
+/* Name of the E-step kernel a context runs ("plain_fp32" / "tc_tf32"). */
+const char *amica_kernel_name(amica_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
