@@ -1,0 +1,385 @@
+"""Benchmark: EM iterations/s of the AMICA engine on one B200 (or N replicas).
+
+Workload (the metric's configuration): n=128 channels, T=1,000,000 samples,
+M=3 models, m=3 mixtures, synthetic FP32 data from cudamica_b200.synth
+(config-2 recipe, seed 0).  A "step" is one full EM iteration over all T
+samples: fused E-step + FP64 M-step.  The sphered data (512 MB) is larger than
+L2 (126 MB), so every step reads it from HBM.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Rank 0 prints one JSON line.  `value` is the mixed-precision (tcgen05 TF32)
+form's iterations/s with the data resident in HBM, timed with CUDA events on
+the engine's stream, max over ranks; the plain FP32 form is timed the same way
+and reported beside it, with both forms' final LL after a fixed-length fit.
+`e2e` runs a whole fit through the public C ABI from pinned host memory.
+`--impl reference` times the reference's own implementation (its CUDA sources
+compiled here for sm_100a, oracle/_ref/cudaamica_ref) on the same workload,
+using its own per-iteration timer.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(n=128, T=1_000_000, M=3, m=3)
+METRIC = "EM iters/s at n=128,T=1M,M=3: mixed-precision vs plain FP32, same final LL"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi") is None:
+            return self
+        fd, self.path = tempfile.mkstemp(prefix="clk_", suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.proc = subprocess.Popen(
+            ["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+             "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        # median under load: ignore idle samples below half of max
+        load = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def make_data(seed: int = 0):
+    from cudamica_b200 import synth
+    d = synth.config2(seed=seed, n=WORKLOAD["n"], T=WORKLOAD["T"], M=WORKLOAD["M"], m=WORKLOAD["m"])
+    A0, c0 = synth.norand_init(WORKLOAD["n"], WORKLOAD["M"])
+    return d.x, A0, c0
+
+
+def new_engine(x, A0, c0, precision, device):
+    from cudamica_b200.engine import Amica
+    eng = Amica(WORKLOAD["n"], WORKLOAD["T"], WORKLOAD["M"], WORKLOAD["m"], precision=precision,
+                device=device, maxiter=4000)
+    eng.load_data(x)
+    eng.preprocess()
+    eng.init(A0, c0)
+    return eng
+
+
+def time_form(x, A0, c0, precision, device, steps, warmup, fit_iters):
+    """Returns (ms per timed step, final LL after fit_iters, estep ms, kernel, launches)."""
+    eng = new_engine(x, A0, c0, precision, device)
+    eng.run(warmup)
+    outs = eng.run(steps)                     # device time via CUDA events on the engine stream
+    ms = float(np.mean([o.device_ms for o in outs]))
+    rest = fit_iters - warmup - steps
+    if rest > 0:
+        outs2 = eng.run(rest)
+        final_ll = outs2[-1].ll
+    else:
+        final_ll = outs[-1].ll
+    est_ms, _ = eng.time_estep(5)
+    kernel = eng.kernel
+    lpi = eng.launches_per_iteration
+    eng.close()
+    return ms, final_ll, est_ms, kernel, lpi
+
+
+def cpu_baseline_port(x, A0, c0, sample_T: int = 100_000):
+    from oracle import oracle as O
+    xs = x[:sample_T].astype(np.float64)
+    xs = xs - xs.mean(0)
+    C = xs.T @ xs / xs.shape[0]
+    d, V = np.linalg.eigh(C)
+    S = (V * (2.0 / np.sqrt(d))) @ V.T
+    xs = xs @ S.T
+    cores = os.cpu_count() or 1
+    orc = O.Oracle(xs, WORKLOAD["M"], WORKLOAD["m"], A0, c0, 0.0, nthreads=cores)
+    orc.step()                                 # warm
+    t0 = time.perf_counter()
+    orc.step()
+    dt = time.perf_counter() - t0
+    scale = WORKLOAD["T"] / sample_T
+    return {"value": 1.0 / (dt * scale), "unit": "iters/s", "cores": cores, "kind": "port",
+            "sample": f"1 EM iteration of the FP64 C oracle on {sample_T} of {WORKLOAD['T']} samples "
+                      f"({dt:.2f} s), scaled x{scale:g}"}
+
+
+def e2e_run(x, A0, c0, device, steps):
+    """Whole fit through the public API from pinned host memory: H2D load,
+    GPU sphering, init, `steps` iterations, D2H of the parameters."""
+    import torch
+    from cudamica_b200.engine import Amica
+    n, T = WORKLOAD["n"], WORKLOAD["T"]
+    # pinned host buffer for the raw data (torch is used only as the allocator)
+    pin = torch.empty((T, n), dtype=torch.float32, pin_memory=True)
+    buf = pin.numpy()
+    buf[...] = x
+    nbytes = x.nbytes
+    pinned = pin.is_pinned()
+    eng = Amica(n, T, WORKLOAD["M"], WORKLOAD["m"], precision=1, device=device, maxiter=4000)
+    t0 = time.perf_counter()
+    eng.load_data(buf)
+    eng.preprocess()
+    eng.init(A0, c0)
+    eng.run(steps)
+    prm = eng.params()
+    dt = time.perf_counter() - t0
+    eng.close()
+    del pin
+    d2h = sum(v.nbytes for v in prm.values()) + steps * 64
+    return {"value": steps / dt, "unit": "iters/s", "h2d_bytes_per_step": nbytes / steps,
+            "d2h_bytes_per_step": d2h / steps, "pinned_host": bool(pinned),
+            "scope": f"load_data + preprocess + init + run({steps}) + get_params, wall clock"}
+
+
+# ---------------------------------------------------------------- reference arm
+def reference_arm(args):
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "cudaamica_ref")
+    if not os.path.exists(ref_bin):
+        return None
+    from cudamica_b200 import synth
+    x, A0, c0 = make_data()
+    n, T, M, m = WORKLOAD["n"], WORKLOAD["T"], WORKLOAD["M"], WORKLOAD["m"]
+    work = tempfile.mkdtemp(prefix="amica_refarm_")
+    try:
+        os.makedirs(os.path.join(work, "datasets"))
+        os.makedirs(os.path.join(work, "out"))
+        x.astype(np.float32).tofile(os.path.join(work, "data.fdt"))
+        xd = x.astype(np.float64)
+        mean = xd.mean(0)
+        xd -= mean
+        C = xd.T @ xd / T
+        dd, V = np.linalg.eigh(C)
+        S = (V * (2.0 / np.sqrt(dd))) @ V.T
+        (xd @ S.T).tofile(os.path.join(work, "datasets", "whitened.fdt"))
+        del xd
+        mean.tofile(os.path.join(work, "datasets", "means.fdt"))
+        A0[0].astype(np.float32).tofile(os.path.join(work, "datasets", "anorand.fdt"))
+        c0[0].astype(np.float32).tofile(os.path.join(work, "datasets", "cnorand.fdt"))
+        A0[1].astype(np.float32).tofile(os.path.join(work, "datasets", "anorand1.fdt"))
+        c0[1].astype(np.float32).tofile(os.path.join(work, "datasets", "cnorand1.fdt"))
+        iters = args.warmup + args.steps
+        lines = ["datafile data.fdt", f"nchannels {n}", f"nsamples {T}", "do_sphere 1",
+                 f"maxiter {iters}", f"nsdm {m}", f"nmmodels {M}", "spherefile out/sphere.fdt",
+                 "block_size 5000", "fix_init on", "do_newton on", "newt_start_iter 50",
+                 "rho_start_iter 1", "update_rho 1"]
+        with open(os.path.join(work, "case.in"), "w") as f:
+            f.write("\n".join(lines) + "\n")
+        env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", "0"))
+        proc = subprocess.run([ref_bin, "-f", "case.in"], cwd=work, capture_output=True, text=True,
+                              timeout=1800, env=env)
+        if proc.returncode != 0:
+            return {"error": f"reference exited {proc.returncode}"}
+        ms = [int(v) for v in re.findall(r"Iteration \d+ times = \d+ ticks, (\d+) ms", proc.stdout)]
+        ll = [float(v) for v in re.findall(r"Iteration \d+: lrate \S+ LL (\S+)", proc.stdout)]
+        timed = ms[args.warmup:]
+        return {"ms": timed, "ll": ll}
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def profile_case(args):
+    """A few E-step launches per form on the first T samples of the workload."""
+    from cudamica_b200.engine import Amica
+    x, A0, c0 = make_data()
+    T = args.T
+    for precision in (1, 0):
+        eng = Amica(WORKLOAD["n"], T, WORKLOAD["M"], WORKLOAD["m"], precision=precision, device=0)
+        eng.load_data(np.ascontiguousarray(x[:T]))
+        eng.preprocess()
+        eng.init(A0, c0)
+        eng.estep_stats()
+        ms, _ = eng.time_estep(2)
+        print(f"{eng.kernel}: {ms:.3f} ms per E-step launch at T={T}")
+        eng.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--fit-iters", type=int, default=200)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="no timing: run a few fused E-step launches of both forms on a "
+                         "T-sample slice (for ncu captures)")
+    ap.add_argument("--T", type=int, default=WORKLOAD["T"])
+    args = ap.parse_args()
+    if args.profile_case:
+        return profile_case(args)
+    ws, rank, local = dist_env()
+    pg = None
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        with Clocks(local) as clk:
+            res = reference_arm(args)
+        if res is None or "error" in res:
+            why = "oracle/_ref/cudaamica_ref not built" if res is None else res["error"]
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return 0
+        ms = float(np.mean(res["ms"])) if res["ms"] else float("nan")
+        v = 1000.0 / ms
+        line = {
+            "impl": "reference", "metric": METRIC, "value": v, "unit": "iters/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "n=128 T=1e6 M=3 m=3, one EM iteration per step", **WORKLOAD,
+                       "l2": "inputs larger than L2 (1 GB FP64 whitened data)",
+                       "implementation": "reference CUDA sources (fp64, cuBLAS + kernels) built "
+                                         "for sm_100a with a MAGMA/MKL stand-in"},
+            "cpu_baseline": {"value": v, "unit": "iters/s", "cores": 1, "kind": "reference",
+                             "sample": f"reference's own per-iteration timer over {len(res['ms'])} "
+                                       "iterations after warm-up; single host thread driving the GPU"},
+            "e2e": {"value": v, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "clocks": clk.summary(),
+            "ll_last": res["ll"][-1] if res["ll"] else None,
+        }
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    device = local
+    torch.cuda.set_device(device)
+    x, A0, c0 = make_data()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    with Clocks(device) as clk:
+        t_mixed, ll_mixed, est_mixed, kname, lpi = time_form(x, A0, c0, 1, device, args.steps,
+                                                             args.warmup, args.fit_iters)
+    clocks = clk.summary()
+    t_plain, ll_plain, est_plain, kname_plain, _ = time_form(x, A0, c0, 0, device, args.steps,
+                                                             args.warmup, args.fit_iters)
+    ms = t_mixed
+    if pg:
+        t = torch.tensor([ms, t_plain], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms, t_plain = float(t[0]), float(t[1])
+    value = ws * 1000.0 / ms
+    hbm, bf16, src = peaks()
+    n, T, M, m = (WORKLOAD[k] for k in ("n", "T", "M", "m"))
+    alg_bytes = 4 * n * T + 4 * M * T            # x read once + Lt write per iteration
+    tc_flops = 4 * M * n * n * T                 # W x and g x^T
+    mufu = (4 * m + 1) * M * n * T
+    achieved_gbs = alg_bytes / (est_mixed * 1e-3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm, "unit": "GB/s",
+            "frac": achieved_gbs / hbm, "traffic": None, "peak_source": f"{src} (MEASURED_PEAKS.json)",
+            "kernel": kname, "kernel_ms": est_mixed, "alg_bytes_per_launch": alg_bytes}
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    mufu_peak = 16 * 148 * sm_mhz * 1e6
+    binding = {"bound": "sfu", "achieved_gops": mufu / (est_mixed * 1e-3) / 1e9,
+               "peak_gops": mufu_peak / 1e9, "frac": (mufu / (est_mixed * 1e-3)) / mufu_peak,
+               "note": "(4m+1)MnT MUFU ops per launch vs 16/clk/SM x 148 SMs at the sampled SM clock",
+               "tensor_tflops": tc_flops / (est_mixed * 1e-3) / 1e12}
+    out = {
+        "metric": METRIC, "value": value, "unit": "iters/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "n=128 T=1e6 M=3 m=3, one EM iteration per step", **WORKLOAD,
+                   "precision": "mixed: tcgen05 TF32 contractions, FP32 densities, FP64 M-step",
+                   "kernel": kname, "l2": "inputs larger than L2 (512 MB sphered data per step)",
+                   "parallelism": "replicas" if ws > 1 else "single GPU"},
+        "plain_fp32": {"value": ws * 1000.0 / t_plain, "ms_per_step": t_plain, "kernel": kname_plain,
+                       "estep_ms": est_plain},
+        "mixed_over_plain": t_plain / ms,
+        "final_ll": {"iters": args.fit_iters, "mixed": ll_mixed, "plain": ll_plain,
+                     "abs_diff": abs(ll_mixed - ll_plain)},
+        "roofline": roof, "roofline_binding": binding,
+        "gpu_launches": lpi * args.steps,
+        "clocks": clocks,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_port(x, A0, c0)
+    if not args.no_e2e:
+        e2e = e2e_run(x, A0, c0, device, args.steps)
+        if pg:
+            t = torch.tensor([e2e["value"]], dtype=torch.float64, device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MIN)
+            e2e["value"] = float(t[0]) * ws
+        out["e2e"] = e2e
+    if rank == 0:
+        print(json.dumps(out))
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -77,7 +77,7 @@ struct EStepArgs {
     const float* Wf;         // M x NP x NP, W[h][i][k] row-major, zero padded
     const float* wc;         // M x NP, (W c)_i in FP32
     const MixParam* mp;      // M x m x NP
-    const float* ltcrel;     // M: log gm_h + ldet_h + ldetS - (same for h = 0)
+    const double* ltc64;     // M: log gm_h + ldet_h + ldetS (FP64)
     const uint8_t* keep;     // T (nullptr = all kept)
     float* Lt_out;           // M x T relative Lt (nullptr = skip)
     float* P_out;            // T relative P (nullptr = skip)
@@ -87,6 +87,28 @@ struct EStepArgs {
     int ldx, n, M, m;
     int ntiles, nclusters;
     int update_rho;
+    int grad_mode;           // 1: beta-denominator slot holds sum u*f'*y for every rho (adjoint)
+};
+
+// Device buffers and host-side settings of the FP64 M-step kernels.
+struct MStepBuffers {
+    double *A, *Anew, *c, *alpha, *mu, *beta, *rho, *gm, *W, *ldet, *ltc64, *aug;
+    double *partial, *raw, *stats, *work, *B, *chunk;
+    int64_t* bflag;
+    int* use_newton;
+    float *Wf, *wcf;
+    MixParam* mp;
+    Ctrl* ctrl;
+    IterRec* hist;
+    int64_t hist_cap;
+    int* err;
+};
+struct MStepCfgHost {
+    int n, m, M, NP;
+    int do_newton, update_rho, rho_start_iter, newt_start_iter, maxdec;
+    int update_gm, update_alpha, update_A, update_mu, update_beta, do_reparm;
+    int do_reject, rejstart, rejint, maxrej;
+    double lratemax, lnatrate, lratefact, rholrate, rhomin, rhomax, rejsig, ldetS;
 };
 
 }  // namespace amica

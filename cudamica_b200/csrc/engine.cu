@@ -1,0 +1,847 @@
+// Host side of the AMICA EM engine: context, device buffers, the iteration
+// pipeline and the C ABI declared in include/amica_b200.h.
+//
+// One iteration is a fixed sequence of kernels on the context's stream:
+//   k_prep (FP64 inverse, log-det, E-step constants)
+//   -> fused E-step (plain FP32 or tcgen05 TF32)
+//   -> k_reduce + k_finalize (deterministic FP64 reduction of per-CTA sums)
+//   -> k_mstep_params -> k_ctrl -> k_mstep_A (-> k_reject on schedule)
+// with no host synchronisation, so amica_run() replays one captured CUDA graph
+// per iteration.  This replaces runamica()'s iteration body
+// (src/amica.cu:820-2541), which synchronised with the host ~T/block_size
+// times per iteration.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "amica_b200.h"
+#include "common.cuh"
+
+namespace amica {
+// estep_plain.cu
+int plain_pad_channels(int n);
+int plain_max_clusters(int n, int m, int M);
+int plain_tile_samples();
+cudaError_t launch_estep_plain(const EStepArgs& a, int NP, int nclusters, cudaStream_t st);
+// estep_tc.cu
+int tc_supported(int n, int m, int M);
+int tc_max_clusters(int n, int m, int M);
+int tc_tile_samples();
+cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStream_t st);
+// preprocess.cu
+cudaError_t launch_preprocess(const float* raw, int64_t T, int n, int do_sphere, double* means,
+                              double* cov, double* sphere, double* evwork, double* ldetS_dev,
+                              float* x, int ldx, cudaStream_t st);
+cudaError_t launch_convert_sphered(const double* xs, int64_t T, int n, float* x, int ldx,
+                                   cudaStream_t st);
+// adjoint.cu
+cudaError_t launch_adjoint(const EStepArgs& a, int NP, double* grad_partial, int nclusters,
+                           cudaStream_t st, bool use_tc);
+cudaError_t launch_adjoint_finalize(const double* grad_partial, double* raw, int nclusters, int n,
+                                    int m, int M, const double* A, const double* c,
+                                    const double* beta, const double* rho, double* out,
+                                    cudaStream_t st);
+
+cudaError_t launch_prep(const MStepBuffers& b, const MStepCfgHost& h, cudaStream_t st);
+cudaError_t launch_reduce_finalize(const MStepBuffers& b, const MStepCfgHost& h, int nclusters,
+                                   cudaStream_t st);
+cudaError_t launch_mstep(const MStepBuffers& b, const MStepCfgHost& h, const float* P_rel,
+                         uint8_t* keep, int64_t T, cudaStream_t st);
+cudaError_t launch_reject_now(const MStepBuffers& b, const MStepCfgHost& h, const float* P_rel,
+                              uint8_t* keep, int64_t T, cudaStream_t st);
+}  // namespace amica
+
+using namespace amica;
+
+struct amica_ctx {
+    amica_cfg cfg{};
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int n = 0, M = 0, m = 0, NP = 0, S = 0;
+    int64_t T = 0;
+    bool use_tc = false;
+    int nclusters = 0, ntiles = 0;
+    bool have_data = false, have_x = false, have_init = false, have_estep = false;
+
+    float* d_rawx = nullptr;     // T x n raw input (float)
+    float* d_x = nullptr;        // T x NP sphered (float)
+    double *d_means = nullptr, *d_sphere = nullptr, *d_cov = nullptr, *d_evwork = nullptr,
+           *d_ldetS = nullptr;
+    double ldetS = 0.0;
+    std::vector<double> h_means, h_sphere;
+
+    MStepBuffers b{};
+    MStepCfgHost hc{};
+    uint8_t* d_keep = nullptr;
+    float *d_Lt = nullptr, *d_P = nullptr;
+    double* d_backup = nullptr;   // parameter snapshot for NaN rollback
+    size_t backup_len = 0;
+    double* d_gradp = nullptr;    // adjoint partials
+    double* d_grad = nullptr;
+
+    Ctrl* h_ctrl = nullptr;       // pinned
+    int* h_err = nullptr;         // pinned
+    std::vector<IterRec> hist;    // host copy of the iteration history
+
+    cudaGraphExec_t graph = nullptr;
+};
+
+namespace {
+
+int g_last_cuda_error = 0;
+
+#define CK(x)                                                                       \
+    do {                                                                            \
+        cudaError_t e_ = (x);                                                       \
+        if (e_ != cudaSuccess) {                                                    \
+            g_last_cuda_error = (int)e_;                                            \
+            if (getenv("AMICA_DEBUG"))                                              \
+                fprintf(stderr, "amica: %s -> %s (%s:%d)\n", #x, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                        \
+            return e_ == cudaErrorMemoryAllocation ? AMICA_ERR_NODEVICEMEM : AMICA_ERR_CUDA; \
+        }                                                                           \
+    } while (0)
+
+template <class T>
+int dalloc(T** p, size_t count) {
+    CK(cudaMalloc((void**)p, sizeof(T) * (count > 0 ? count : 1)));
+    CK(cudaMemset(*p, 0, sizeof(T) * (count > 0 ? count : 1)));
+    return AMICA_OK;
+}
+
+#define TRY(x)                    \
+    do {                          \
+        int r_ = (x);             \
+        if (r_ != AMICA_OK) return r_; \
+    } while (0)
+
+int64_t param_len(const amica_ctx* c) {
+    const int64_t n = c->n, M = c->M, m = c->m;
+    return M * n * n + M * n + 4 * M * m * n + M;
+}
+
+int snapshot_params(amica_ctx* c, bool restore) {
+    const int64_t n = c->n, M = c->M, m = c->m;
+    double* p = c->d_backup;
+    struct Seg { double* d; int64_t len; } segs[] = {
+        {c->b.A, M * n * n}, {c->b.c, M * n}, {c->b.alpha, M * m * n}, {c->b.mu, M * m * n},
+        {c->b.beta, M * m * n}, {c->b.rho, M * m * n}, {c->b.gm, M}};
+    for (auto& s : segs) {
+        if (restore) CK(cudaMemcpyAsync(s.d, p, sizeof(double) * s.len, cudaMemcpyDeviceToDevice, c->st));
+        else CK(cudaMemcpyAsync(p, s.d, sizeof(double) * s.len, cudaMemcpyDeviceToDevice, c->st));
+        p += s.len;
+    }
+    Ctrl* cb = reinterpret_cast<Ctrl*>(p);
+    if (restore) CK(cudaMemcpyAsync(c->b.ctrl, cb, sizeof(Ctrl), cudaMemcpyDeviceToDevice, c->st));
+    else CK(cudaMemcpyAsync(cb, c->b.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToDevice, c->st));
+    return AMICA_OK;
+}
+
+EStepArgs estep_args(amica_ctx* c) {
+    EStepArgs a{};
+    a.x = c->d_x;
+    a.Wf = c->b.Wf;
+    a.wc = c->b.wcf;
+    a.mp = c->b.mp;
+    a.ltc64 = c->b.ltc64;
+    a.keep = c->d_keep;
+    a.Lt_out = c->d_Lt;
+    a.P_out = c->d_P;
+    a.partial = c->b.partial;
+    a.err = c->b.err;
+    a.T = c->T;
+    a.ldx = c->NP;
+    a.n = c->n;
+    a.M = c->M;
+    a.m = c->m;
+    a.ntiles = c->ntiles;
+    a.nclusters = c->nclusters;
+    a.update_rho = (int)c->cfg.update_rho;
+    return a;
+}
+
+int enqueue_estep(amica_ctx* c) {
+    CK(launch_prep(c->b, c->hc, c->st));
+    EStepArgs a = estep_args(c);
+    if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st));
+    else CK(launch_estep_plain(a, c->NP, c->nclusters, c->st));
+    CK(launch_reduce_finalize(c->b, c->hc, c->nclusters, c->st));
+    return AMICA_OK;
+}
+
+// Kernels one iteration launches: prep, E-step, reduce, finalize, params, ctrl,
+// A update (+ rejection when enabled).
+int launches_per_iteration(const amica_ctx* c) { return 7 + (c->hc.do_reject ? 1 : 0); }
+
+int enqueue_iteration(amica_ctx* c) {
+    TRY(enqueue_estep(c));
+    CK(launch_mstep(c->b, c->hc, c->d_P, c->d_keep, c->T, c->st));
+    return AMICA_OK;
+}
+
+int check_device_error(amica_ctx* c) {
+    CK(cudaMemcpyAsync(c->h_err, c->b.err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    int e = *c->h_err;
+    if (e) {
+        CK(cudaMemsetAsync(c->b.err, 0, sizeof(int), c->st));
+        if (e & kErrWaitTimeout) return AMICA_ERR_TIMEOUT;
+        if (e & kErrSingular) return AMICA_ERR_SINGULAR;
+        if (e & kErrShape) return AMICA_ERR_UNSUPPORTED;
+        return AMICA_ERR_CUDA;
+    }
+    return AMICA_OK;
+}
+
+void fill_out(const IterRec& r, const Ctrl& c, double ms, amica_iter_out* out) {
+    if (!out) return;
+    out->iter = r.iter;
+    out->ll = r.ll;
+    out->lrate = r.lrate;
+    out->ll_decreased = r.ll_decreased;
+    out->newton = r.newton;
+    out->nkeep = c.nkeep;
+    out->nrejected = r.nrejected;
+    out->device_ms = ms;
+}
+
+void print_iter(const amica_ctx* c, const IterRec& r) {
+    if (!c->cfg.verbose) return;
+    // the reference's stdout lines, src/amica.cu:1983-1986 and :2322-2324
+    fprintf(stdout, "Iteration %ld: lrate %.16f LL %.16f \n", (long)r.iter, r.lrate, r.ll);
+    if (r.ll_decreased) fprintf(stdout, "Likelihood decreasing!\n");
+    if (r.nrejected) fprintf(stdout, "Rejected %ld samples\n", (long)r.nrejected);
+}
+
+}  // namespace
+
+extern "C" {
+
+int amica_default_cfg(amica_cfg* c) {
+    if (!c) return AMICA_ERR_INVALIDPARAM;
+    memset(c, 0, sizeof(*c));
+    c->nmmodels = 1;          // include/config.h:46-83
+    c->nsdm = 3;
+    c->maxiter = 200;
+    c->do_sphere = 1;
+    c->block_size = 5000;
+    c->fix_init = 1;
+    c->do_newton = 1;
+    c->update_rho = 1;
+    c->rho_start_iter = 1;
+    c->newt_start_iter = 50;
+    c->maxdec = 3;
+    c->update_gm = c->update_alpha = c->update_A = c->update_mu = c->update_beta = 1;
+    c->do_reparm = 1;
+    c->do_reject = 0;
+    c->rejstart = 10;
+    c->rejint = 10;
+    c->maxrej = 100;
+    c->precision = AMICA_PREC_MIXED;
+    c->device = 0;
+    c->seed = 1234;
+    c->verbose = 0;
+    c->lrate0 = 0.1;
+    c->lratemax = 1.0;
+    c->lnatrate = 0.1;
+    c->lratefact = 0.5;
+    c->rho0 = 1.5;
+    c->rholrate = 0.1;
+    c->rhomin = 1.0;
+    c->rhomax = 2.0;
+    c->rejsig = 3.0;
+    return AMICA_OK;
+}
+
+int64_t amica_stats_len(int64_t n, int64_t M, int64_t m) {
+    return 1 + M * (1 + 2 * n + n * n + 7 * m * n);
+}
+
+const char* amica_status_string(int s) {
+    switch (s) {
+        case AMICA_OK: return "Success!";
+        case AMICA_ERR_NODEVICEMEM: return "No device memory";
+        case AMICA_ERR_NOPARAM: return "No parameter";
+        case AMICA_ERR_INVALIDPARAM: return "Invalid parameter";
+        case AMICA_ERR_INVALIDCONFIG: return "Invalid config";
+        case AMICA_ERR_NOFILE: return "No file";
+        case AMICA_ERR_IO: return "Input/Output error";
+        case AMICA_ERR_NOMEM: return "No more memory on host";
+        case AMICA_ERR_CUDA: return "CUDA runtime error";
+        case AMICA_ERR_STATE: return "Call out of order";
+        case AMICA_ERR_SINGULAR: return "Mixing matrix is singular";
+        case AMICA_ERR_NUMERIC: return "Non-finite log-likelihood or parameters (state rolled back)";
+        case AMICA_ERR_TIMEOUT: return "A bounded device-side wait expired";
+        case AMICA_ERR_UNSUPPORTED: return "Shape not supported by the compiled kernels";
+        case AMICA_ERR_NODEVICE: return "No usable CUDA device";
+        default: return "Unknown error";
+    }
+}
+
+int amica_create(const amica_cfg* cfg, amica_ctx** out) {
+    if (!cfg || !out) return AMICA_ERR_INVALIDPARAM;
+    *out = nullptr;
+    const int64_t n = cfg->nchannels, T = cfg->nsamples, M = cfg->nmmodels, m = cfg->nsdm;
+    if (n < 2 || T < 2 || M < 1 || m < 1) return AMICA_ERR_INVALIDPARAM;
+    if (M > kMaxModels || m > 5) return AMICA_ERR_UNSUPPORTED;
+    if (cfg->precision != AMICA_PREC_FP32 && cfg->precision != AMICA_PREC_MIXED)
+        return AMICA_ERR_INVALIDPARAM;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return AMICA_ERR_NODEVICE;
+    if (cfg->device < 0 || cfg->device >= ndev) return AMICA_ERR_INVALIDPARAM;
+    const int NP = plain_pad_channels((int)n);
+    if (NP < 0) return AMICA_ERR_UNSUPPORTED;
+
+    amica_ctx* c = new amica_ctx();
+    c->cfg = *cfg;
+    c->dev = (int)cfg->device;
+    c->n = (int)n; c->T = T; c->M = (int)M; c->m = (int)m; c->NP = NP;
+    CK(cudaSetDevice(c->dev));
+    CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&c->ev0));
+    CK(cudaEventCreate(&c->ev1));
+
+    c->use_tc = (cfg->precision == AMICA_PREC_MIXED) && tc_supported((int)n, (int)m, (int)M);
+    c->S = c->use_tc ? tc_tile_samples() : plain_tile_samples();
+    c->ntiles = (int)((T + c->S - 1) / c->S);
+    int maxcl = c->use_tc ? tc_max_clusters((int)n, (int)m, (int)M) : plain_max_clusters((int)n, (int)m, (int)M);
+    if (maxcl <= 0) { amica_destroy(c); return AMICA_ERR_UNSUPPORTED; }
+    c->nclusters = maxcl < c->ntiles ? maxcl : c->ntiles;
+
+    MStepCfgHost& h = c->hc;
+    h.n = (int)n; h.m = (int)m; h.M = (int)M; h.NP = NP;
+    h.do_newton = (int)cfg->do_newton; h.update_rho = (int)cfg->update_rho;
+    h.rho_start_iter = (int)cfg->rho_start_iter; h.newt_start_iter = (int)cfg->newt_start_iter;
+    h.maxdec = (int)cfg->maxdec; h.update_gm = (int)cfg->update_gm;
+    h.update_alpha = (int)cfg->update_alpha; h.update_A = (int)cfg->update_A;
+    h.update_mu = (int)cfg->update_mu; h.update_beta = (int)cfg->update_beta;
+    h.do_reparm = (int)cfg->do_reparm; h.do_reject = (int)cfg->do_reject;
+    h.rejstart = (int)cfg->rejstart; h.rejint = (int)cfg->rejint; h.maxrej = (int)cfg->maxrej;
+    h.lratemax = cfg->lratemax; h.lnatrate = cfg->lnatrate; h.lratefact = cfg->lratefact;
+    h.rholrate = cfg->rholrate; h.rhomin = cfg->rhomin; h.rhomax = cfg->rhomax;
+    h.rejsig = cfg->rejsig; h.ldetS = 0.0;
+
+    MStepBuffers& b = c->b;
+    const size_t nn = (size_t)n * n, mn = (size_t)m * n;
+    int r = AMICA_OK;
+#define AL(p, cnt) if ((r = dalloc(&(p), (cnt))) != AMICA_OK) { amica_destroy(c); return r; }
+    AL(b.A, M * nn); AL(b.Anew, M * nn); AL(b.c, M * n); AL(b.alpha, M * mn); AL(b.mu, M * mn);
+    AL(b.beta, M * mn); AL(b.rho, M * mn); AL(b.gm, M); AL(b.W, M * nn); AL(b.ldet, M);
+    AL(b.ltc64, M); AL(b.aug, M * nn * 2);
+    PartLayout PL{(int)n, (int)m};
+    AL(b.partial, (size_t)c->nclusters * M * PL.stride());
+    AL(b.raw, M * (size_t)PL.stride());
+    AL(b.stats, (size_t)amica_stats_len(n, M, m));
+    AL(b.work, M * 4 * n); AL(b.B, M * nn);
+    const int64_t nch = (T + 4095) / 4096;
+    AL(b.chunk, 2 * nch + 2);
+    AL(b.bflag, M); AL(b.use_newton, M);
+    AL(b.Wf, (size_t)M * NP * NP); AL(b.wcf, (size_t)M * NP); AL(b.mp, (size_t)M * m * NP);
+    AL(b.ctrl, 1);
+    b.hist_cap = cfg->maxiter > 0 ? cfg->maxiter : 200;
+    if (b.hist_cap < 1000) b.hist_cap = 1000;
+    AL(b.hist, b.hist_cap);
+    AL(b.err, 1);
+    AL(c->d_keep, T); AL(c->d_Lt, M * T); AL(c->d_P, T);
+    AL(c->d_x, (size_t)T * NP);
+    AL(c->d_means, n); AL(c->d_sphere, nn); AL(c->d_cov, nn); AL(c->d_evwork, 4 * nn + 4 * n);
+    AL(c->d_ldetS, 1);
+    c->backup_len = param_len(c) + (sizeof(Ctrl) + 7) / 8;
+    AL(c->d_backup, c->backup_len);
+#undef AL
+    CK(cudaMemsetAsync(c->d_keep, 1, T, c->st));
+    CK(cudaMallocHost(&c->h_ctrl, sizeof(Ctrl)));
+    CK(cudaMallocHost(&c->h_err, sizeof(int)));
+    CK(cudaStreamSynchronize(c->st));
+    *out = c;
+    return AMICA_OK;
+}
+
+int amica_destroy(amica_ctx* c) {
+    if (!c) return AMICA_OK;
+    cudaSetDevice(c->dev);
+    if (c->st) cudaStreamSynchronize(c->st);
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    void* ptrs[] = {c->b.A, c->b.Anew, c->b.c, c->b.alpha, c->b.mu, c->b.beta, c->b.rho, c->b.gm,
+                    c->b.W, c->b.ldet, c->b.ltc64, c->b.aug, c->b.partial, c->b.raw, c->b.stats,
+                    c->b.work, c->b.B, c->b.chunk, c->b.bflag, c->b.use_newton, c->b.Wf, c->b.wcf,
+                    c->b.mp, c->b.ctrl, c->b.hist, c->b.err, c->d_keep, c->d_Lt, c->d_P, c->d_x,
+                    c->d_rawx, c->d_means, c->d_sphere, c->d_cov, c->d_evwork, c->d_ldetS,
+                    c->d_backup, c->d_gradp, c->d_grad};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (c->h_ctrl) cudaFreeHost(c->h_ctrl);
+    if (c->h_err) cudaFreeHost(c->h_err);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+    return AMICA_OK;
+}
+
+const char* amica_kernel_name(amica_ctx* c) {
+    if (!c) return "";
+    return c->use_tc ? "tc_tf32" : "plain_fp32";
+}
+
+static int load_raw(amica_ctx* c, const float* x, int64_t n, int64_t T, cudaMemcpyKind kind) {
+    if (!c || !x) return AMICA_ERR_INVALIDPARAM;
+    if (n != c->n || T != c->T) return AMICA_ERR_INVALIDPARAM;
+    CK(cudaSetDevice(c->dev));
+    if (!c->d_rawx) CK(cudaMalloc(&c->d_rawx, sizeof(float) * (size_t)T * n));
+    CK(cudaMemcpyAsync(c->d_rawx, x, sizeof(float) * (size_t)T * n, kind, c->st));
+    c->have_data = true;
+    c->have_x = false;
+    return AMICA_OK;
+}
+
+int amica_load_data(amica_ctx* c, const float* x, int64_t n, int64_t T) {
+    return load_raw(c, x, n, T, cudaMemcpyHostToDevice);
+}
+
+int amica_load_data_device(amica_ctx* c, const float* dx, int64_t n, int64_t T) {
+    return load_raw(c, dx, n, T, cudaMemcpyDeviceToDevice);
+}
+
+int amica_preprocess(amica_ctx* c) {
+    if (!c) return AMICA_ERR_INVALIDPARAM;
+    if (!c->have_data) return AMICA_ERR_STATE;
+    CK(cudaSetDevice(c->dev));
+    CK(launch_preprocess(c->d_rawx, c->T, c->n, (int)c->cfg.do_sphere, c->d_means, c->d_cov,
+                         c->d_sphere, c->d_evwork, c->d_ldetS, c->d_x, c->NP, c->st));
+    double ld = 0.0;
+    CK(cudaMemcpyAsync(&ld, c->d_ldetS, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    TRY(check_device_error(c));
+    c->ldetS = ld;
+    c->hc.ldetS = ld;
+    c->have_x = true;
+    return AMICA_OK;
+}
+
+int amica_set_sphered(amica_ctx* c, const double* xs, const double* means, const double* sphere,
+                      double ldetS) {
+    if (!c || !xs) return AMICA_ERR_INVALIDPARAM;
+    CK(cudaSetDevice(c->dev));
+    double* tmp = nullptr;
+    const size_t bytes = sizeof(double) * (size_t)c->T * c->n;
+    CK(cudaMalloc(&tmp, bytes));
+    CK(cudaMemcpyAsync(tmp, xs, bytes, cudaMemcpyHostToDevice, c->st));
+    CK(launch_convert_sphered(tmp, c->T, c->n, c->d_x, c->NP, c->st));
+    if (means) CK(cudaMemcpyAsync(c->d_means, means, sizeof(double) * c->n, cudaMemcpyHostToDevice, c->st));
+    if (sphere) CK(cudaMemcpyAsync(c->d_sphere, sphere, sizeof(double) * c->n * c->n, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaFree(tmp));
+    c->ldetS = ldetS;
+    c->hc.ldetS = ldetS;
+    c->have_x = true;
+    return AMICA_OK;
+}
+
+int amica_init(amica_ctx* c, const double* A0, const double* c0) {
+    if (!c) return AMICA_ERR_INVALIDPARAM;
+    CK(cudaSetDevice(c->dev));
+    const int n = c->n, M = c->M, m = c->m;
+    std::vector<double> A((size_t)M * n * n), cc((size_t)M * n), alpha((size_t)M * m * n),
+        mu((size_t)M * m * n), beta((size_t)M * m * n), rho((size_t)M * m * n), gm(M);
+    std::mt19937_64 rng((uint64_t)c->cfg.seed);
+    std::uniform_real_distribution<double> U(0.0, 1.0);
+    std::normal_distribution<double> N01(0.0, 1.0);
+    if (A0) {
+        memcpy(A.data(), A0, sizeof(double) * A.size());
+        if (c0) memcpy(cc.data(), c0, sizeof(double) * cc.size());
+    } else {
+        // A = I + 0.05 (U - 0.5), unit columns; c ~ N(0, 1) (src/amica.cu:272-312)
+        for (int h = 0; h < M; h++) {
+            double* Ah = A.data() + (size_t)h * n * n;
+            for (int e = 0; e < n * n; e++) Ah[e] = (U(rng) - 0.5) * 0.05 + ((e % n) == (e / n) ? 1.0 : 0.0);
+            for (int col = 0; col < n; col++) {
+                double s = 0.0;
+                for (int r = 0; r < n; r++) s += Ah[col * n + r] * Ah[col * n + r];
+                s = sqrt(s);
+                for (int r = 0; r < n; r++) Ah[col * n + r] /= s;
+            }
+            for (int i = 0; i < n; i++) cc[(size_t)h * n + i] = c0 ? c0[(size_t)h * n + i] : N01(rng);
+        }
+    }
+    for (int h = 0; h < M; h++) {
+        gm[h] = 1.0 / M;                               // src/amica.cu:337
+        for (int j = 0; j < m; j++)
+            for (int i = 0; i < n; i++) {
+                const size_t idx = ((size_t)h * m + j) * n + i;
+                alpha[idx] = 1.0 / m;                  // :339-345
+                if (c->cfg.fix_init) {                 // :347-362
+                    mu[idx] = (double)j - (m - 1.0) / 2.0;
+                    beta[idx] = 1.0;
+                } else {                               // :363-387
+                    mu[idx] = (m > 1) ? 0.1 * N01(rng) : 0.0;
+                    beta[idx] = 1.0 + 0.1 * N01(rng);
+                }
+                rho[idx] = c->cfg.rho0;                // :389-394
+            }
+    }
+    CK(cudaMemcpyAsync(c->b.A, A.data(), sizeof(double) * A.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->b.c, cc.data(), sizeof(double) * cc.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->b.alpha, alpha.data(), sizeof(double) * alpha.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->b.mu, mu.data(), sizeof(double) * mu.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->b.beta, beta.data(), sizeof(double) * beta.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->b.rho, rho.data(), sizeof(double) * rho.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->b.gm, gm.data(), sizeof(double) * gm.size(), cudaMemcpyHostToDevice, c->st));
+    Ctrl ctl{};
+    ctl.lrate = c->cfg.lrate0;
+    ctl.lratemax = c->cfg.lratemax;
+    ctl.iter = 0;
+    ctl.nkeep = c->T;
+    *c->h_ctrl = ctl;
+    CK(cudaMemcpyAsync(c->b.ctrl, c->h_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemsetAsync(c->d_keep, 1, c->T, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->hist.clear();
+    c->have_init = true;
+    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+    return AMICA_OK;
+}
+
+int amica_em_step(amica_ctx* c, amica_iter_out* out) {
+    if (!c) return AMICA_ERR_INVALIDPARAM;
+    if (!c->have_x || !c->have_init) return AMICA_ERR_STATE;
+    CK(cudaSetDevice(c->dev));
+    TRY(snapshot_params(c, false));
+    CK(cudaEventRecord(c->ev0, c->st));
+    TRY(enqueue_iteration(c));
+    CK(cudaEventRecord(c->ev1, c->st));
+    CK(cudaMemcpyAsync(c->h_ctrl, c->b.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->have_estep = true;
+    int e = check_device_error(c);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    const Ctrl ctl = *c->h_ctrl;
+    if (e == AMICA_OK && !std::isfinite(ctl.ll)) e = AMICA_ERR_NUMERIC;
+    if (e != AMICA_OK) {
+        snapshot_params(c, true);
+        cudaStreamSynchronize(c->st);
+        return e;
+    }
+    IterRec r{};
+    CK(cudaMemcpy(&r, c->b.hist + (ctl.iter - 1), sizeof(IterRec), cudaMemcpyDeviceToHost));
+    c->hist.push_back(r);
+    print_iter(c, r);
+    fill_out(r, ctl, ms, out);
+    return AMICA_OK;
+}
+
+int amica_run(amica_ctx* c, int64_t maxiter, amica_iter_out* hist) {
+    if (!c) return AMICA_ERR_INVALIDPARAM;
+    if (!c->have_x || !c->have_init) return AMICA_ERR_STATE;
+    if (maxiter < 0) return AMICA_ERR_INVALIDPARAM;
+    CK(cudaSetDevice(c->dev));
+    if (!c->graph) {
+        // warm launch outside capture (sets kernel attributes), then capture
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+        int r = enqueue_iteration(c);
+        cudaError_t ce = cudaStreamEndCapture(c->st, &g);
+        if (r != AMICA_OK) return r;
+        CK(ce);
+        CK(cudaGraphInstantiate(&c->graph, g, 0));
+        CK(cudaGraphDestroy(g));
+    }
+    CK(cudaMemcpyAsync(c->h_ctrl, c->b.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    const int64_t it0 = c->h_ctrl->iter;
+    if (it0 + maxiter > c->b.hist_cap) return AMICA_ERR_INVALIDPARAM;
+    TRY(snapshot_params(c, false));
+    CK(cudaEventRecord(c->ev0, c->st));
+    for (int64_t k = 0; k < maxiter; k++) CK(cudaGraphLaunch(c->graph, c->st));
+    CK(cudaEventRecord(c->ev1, c->st));
+    CK(cudaMemcpyAsync(c->h_ctrl, c->b.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->have_estep = maxiter > 0 || c->have_estep;
+    int e = check_device_error(c);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    std::vector<IterRec> recs(maxiter);
+    if (maxiter > 0)
+        CK(cudaMemcpy(recs.data(), c->b.hist + it0, sizeof(IterRec) * maxiter, cudaMemcpyDeviceToHost));
+    for (int64_t k = 0; k < maxiter; k++) {
+        if (e == AMICA_OK && !std::isfinite(recs[k].ll)) e = AMICA_ERR_NUMERIC;
+        c->hist.push_back(recs[k]);
+        print_iter(c, recs[k]);
+        if (hist) fill_out(recs[k], *c->h_ctrl, maxiter ? ms / maxiter : 0.0, &hist[k]);
+    }
+    if (e == AMICA_ERR_NUMERIC) {
+        snapshot_params(c, true);
+        cudaStreamSynchronize(c->st);
+    }
+    return e;
+}
+
+int amica_get_params(amica_ctx* c, double* A, double* W, double* cc, double* gm, double* alpha,
+                     double* mu, double* beta, double* rho) {
+    if (!c) return AMICA_ERR_INVALIDPARAM;
+    CK(cudaSetDevice(c->dev));
+    const size_t nn = (size_t)c->n * c->n * c->M, mn = (size_t)c->m * c->n * c->M;
+    if (A) CK(cudaMemcpyAsync(A, c->b.A, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->st));
+    if (W) CK(cudaMemcpyAsync(W, c->b.W, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->st));
+    if (cc) CK(cudaMemcpyAsync(cc, c->b.c, sizeof(double) * c->n * c->M, cudaMemcpyDeviceToHost, c->st));
+    if (gm) CK(cudaMemcpyAsync(gm, c->b.gm, sizeof(double) * c->M, cudaMemcpyDeviceToHost, c->st));
+    if (alpha) CK(cudaMemcpyAsync(alpha, c->b.alpha, sizeof(double) * mn, cudaMemcpyDeviceToHost, c->st));
+    if (mu) CK(cudaMemcpyAsync(mu, c->b.mu, sizeof(double) * mn, cudaMemcpyDeviceToHost, c->st));
+    if (beta) CK(cudaMemcpyAsync(beta, c->b.beta, sizeof(double) * mn, cudaMemcpyDeviceToHost, c->st));
+    if (rho) CK(cudaMemcpyAsync(rho, c->b.rho, sizeof(double) * mn, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return AMICA_OK;
+}
+
+int amica_set_params(amica_ctx* c, const double* A, const double* cc, const double* gm,
+                     const double* alpha, const double* mu, const double* beta, const double* rho) {
+    if (!c) return AMICA_ERR_INVALIDPARAM;
+    CK(cudaSetDevice(c->dev));
+    const size_t nn = (size_t)c->n * c->n * c->M, mn = (size_t)c->m * c->n * c->M;
+    if (A) CK(cudaMemcpyAsync(c->b.A, A, sizeof(double) * nn, cudaMemcpyHostToDevice, c->st));
+    if (cc) CK(cudaMemcpyAsync(c->b.c, cc, sizeof(double) * c->n * c->M, cudaMemcpyHostToDevice, c->st));
+    if (gm) CK(cudaMemcpyAsync(c->b.gm, gm, sizeof(double) * c->M, cudaMemcpyHostToDevice, c->st));
+    if (alpha) CK(cudaMemcpyAsync(c->b.alpha, alpha, sizeof(double) * mn, cudaMemcpyHostToDevice, c->st));
+    if (mu) CK(cudaMemcpyAsync(c->b.mu, mu, sizeof(double) * mn, cudaMemcpyHostToDevice, c->st));
+    if (beta) CK(cudaMemcpyAsync(c->b.beta, beta, sizeof(double) * mn, cudaMemcpyHostToDevice, c->st));
+    if (rho) CK(cudaMemcpyAsync(c->b.rho, rho, sizeof(double) * mn, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return AMICA_OK;
+}
+
+int amica_estep_stats(amica_ctx* c, double* stats) {
+    if (!c) return AMICA_ERR_INVALIDPARAM;
+    if (!c->have_x || !c->have_init) return AMICA_ERR_STATE;
+    CK(cudaSetDevice(c->dev));
+    TRY(enqueue_estep(c));
+    c->have_estep = true;
+    TRY(check_device_error(c));
+    if (stats)
+        CK(cudaMemcpy(stats, c->b.stats, sizeof(double) * amica_stats_len(c->n, c->M, c->m),
+                      cudaMemcpyDeviceToHost));
+    return AMICA_OK;
+}
+
+int amica_get_loglik(amica_ctx* c, double* Lt, double* P, uint8_t* keep) {
+    if (!c) return AMICA_ERR_INVALIDPARAM;
+    if (!c->have_estep) return AMICA_ERR_STATE;
+    CK(cudaSetDevice(c->dev));
+    CK(cudaStreamSynchronize(c->st));
+    double ltc0 = 0.0;
+    CK(cudaMemcpy(&ltc0, c->b.ltc64, sizeof(double), cudaMemcpyDeviceToHost));
+    if (Lt || P) {
+        const int64_t len = (Lt ? (int64_t)c->M : 0) * c->T;
+        std::vector<float> tmp(len > c->T ? len : c->T);
+        if (Lt) {
+            CK(cudaMemcpy(tmp.data(), c->d_Lt, sizeof(float) * c->M * c->T, cudaMemcpyDeviceToHost));
+            for (int64_t e = 0; e < (int64_t)c->M * c->T; e++) Lt[e] = (double)tmp[e] + ltc0;
+        }
+        if (P) {
+            CK(cudaMemcpy(tmp.data(), c->d_P, sizeof(float) * c->T, cudaMemcpyDeviceToHost));
+            for (int64_t t = 0; t < c->T; t++) P[t] = (double)tmp[t] + ltc0;
+        }
+    }
+    if (keep) CK(cudaMemcpy(keep, c->d_keep, c->T, cudaMemcpyDeviceToHost));
+    return AMICA_OK;
+}
+
+// Relative per-sample P as the kernels store it (float), for bit-exact checks.
+int amica_get_p_relative(amica_ctx* c, float* P) {
+    if (!c || !P) return AMICA_ERR_INVALIDPARAM;
+    CK(cudaSetDevice(c->dev));
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaMemcpy(P, c->d_P, sizeof(float) * c->T, cudaMemcpyDeviceToHost));
+    return AMICA_OK;
+}
+
+int amica_reject_now(amica_ctx* c, int64_t* nrej) {
+    if (!c) return AMICA_ERR_INVALIDPARAM;
+    if (!c->have_estep) return AMICA_ERR_STATE;
+    CK(cudaSetDevice(c->dev));
+    CK(launch_reject_now(c->b, c->hc, c->d_P, c->d_keep, c->T, c->st));
+    CK(cudaMemcpyAsync(c->h_ctrl, c->b.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (nrej) *nrej = c->h_ctrl->last_rejected;
+    return AMICA_OK;
+}
+
+int amica_loglik_adjoint(amica_ctx* c, double* ll, double* dW, double* dmu, double* dbeta,
+                         double* drho) {
+    if (!c) return AMICA_ERR_INVALIDPARAM;
+    if (!c->have_x || !c->have_init) return AMICA_ERR_STATE;
+    CK(cudaSetDevice(c->dev));
+    const int n = c->n, M = c->M, m = c->m;
+    const size_t glen = 1 + (size_t)M * n * n + 3 * (size_t)M * m * n;
+    if (!c->d_grad) CK(cudaMalloc(&c->d_grad, sizeof(double) * glen));
+    CK(launch_prep(c->b, c->hc, c->st));
+    EStepArgs a = estep_args(c);
+    CK(launch_adjoint(a, c->NP, c->b.partial, c->nclusters, c->st, c->use_tc));
+    CK(launch_adjoint_finalize(c->b.partial, c->b.raw, c->nclusters, n, m, M, c->b.A, c->b.c,
+                               c->b.beta, c->b.rho, c->d_grad, c->st));
+    TRY(check_device_error(c));
+    std::vector<double> g(glen);
+    CK(cudaMemcpy(g.data(), c->d_grad, sizeof(double) * glen, cudaMemcpyDeviceToHost));
+    // L = sum_t P(t) / (n T_kept): add the constant part T_kept * ltc0
+    double ltc0 = 0.0;
+    CK(cudaMemcpy(&ltc0, c->b.ltc64, sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(c->h_ctrl, c->b.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+    const double Tk = (double)c->h_ctrl->nkeep;
+    const double norm = 1.0 / ((double)n * Tk);
+    if (ll) *ll = (g[0] + Tk * ltc0) * norm;
+    size_t off = 1;
+    if (dW) for (size_t e = 0; e < (size_t)M * n * n; e++) dW[e] = g[off + e] * norm;
+    off += (size_t)M * n * n;
+    if (dmu) for (size_t e = 0; e < (size_t)M * m * n; e++) dmu[e] = g[off + e] * norm;
+    off += (size_t)M * m * n;
+    if (dbeta) for (size_t e = 0; e < (size_t)M * m * n; e++) dbeta[e] = g[off + e] * norm;
+    off += (size_t)M * m * n;
+    if (drho) for (size_t e = 0; e < (size_t)M * m * n; e++) drho[e] = g[off + e] * norm;
+    return AMICA_OK;
+}
+
+static int write_doubles(const char* path, const double* v, size_t count) {
+    FILE* f = fopen(path, "w");
+    if (!f) return AMICA_ERR_NOFILE;
+    const size_t w = fwrite(v, sizeof(double), count, f);
+    fclose(f);
+    return w == count ? AMICA_OK : AMICA_ERR_IO;
+}
+
+int amica_write_outputs(amica_ctx* c, const amica_paths* p) {
+    if (!c || !p) return AMICA_ERR_INVALIDPARAM;
+    if (!c->have_init) return AMICA_ERR_STATE;
+    const int n = c->n, M = c->M, m = c->m;
+    const size_t nn = (size_t)n * n;
+    std::vector<double> A(M * nn), W(M * nn), cc(M * n), gm(M), alpha(M * m * n), mu(M * m * n),
+        beta(M * m * n), rho(M * m * n), S(nn), means(n);
+    TRY(amica_get_params(c, A.data(), W.data(), cc.data(), gm.data(), alpha.data(), mu.data(),
+                         beta.data(), rho.data()));
+    CK(cudaMemcpy(S.data(), c->d_sphere, sizeof(double) * nn, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(means.data(), c->d_means, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    // back-transform to the unsphered space as src/amica.cu:2564-2668 does:
+    // c <- S^+ c + mean, A <- S^+ A with unit columns (mu/beta left as stored)
+    std::vector<double> Sinv(nn);
+    {
+        // S^{-1} by Gauss-Jordan on the host (n x n output-stage algebra)
+        std::vector<double> a(nn * 2);
+        for (int r = 0; r < n; r++)
+            for (int col = 0; col < 2 * n; col++)
+                a[(size_t)r * 2 * n + col] = col < n ? S[(size_t)col * n + r] : (col - n == r ? 1.0 : 0.0);
+        for (int k = 0; k < n; k++) {
+            int pv = k;
+            for (int r = k + 1; r < n; r++)
+                if (fabs(a[(size_t)r * 2 * n + k]) > fabs(a[(size_t)pv * 2 * n + k])) pv = r;
+            if (a[(size_t)pv * 2 * n + k] == 0.0) return AMICA_ERR_SINGULAR;
+            if (pv != k)
+                for (int col = 0; col < 2 * n; col++) std::swap(a[(size_t)k * 2 * n + col], a[(size_t)pv * 2 * n + col]);
+            const double inv = 1.0 / a[(size_t)k * 2 * n + k];
+            for (int col = 0; col < 2 * n; col++) a[(size_t)k * 2 * n + col] *= inv;
+            for (int r = 0; r < n; r++) {
+                if (r == k) continue;
+                const double f = a[(size_t)r * 2 * n + k];
+                if (f != 0.0)
+                    for (int col = 0; col < 2 * n; col++) a[(size_t)r * 2 * n + col] -= f * a[(size_t)k * 2 * n + col];
+            }
+        }
+        for (int r = 0; r < n; r++)
+            for (int col = 0; col < n; col++) Sinv[(size_t)col * n + r] = a[(size_t)r * 2 * n + n + col];
+    }
+    std::vector<double> Aout(M * nn), cout_(M * n);
+    for (int h = 0; h < M; h++) {
+        for (int i = 0; i < n; i++) {
+            double acc = means[i];
+            for (int k = 0; k < n; k++) acc += Sinv[(size_t)k * n + i] * cc[(size_t)h * n + k];
+            cout_[(size_t)h * n + i] = acc;
+        }
+        for (int col = 0; col < n; col++) {
+            double s2 = 0.0;
+            for (int r = 0; r < n; r++) {
+                double acc = 0.0;
+                for (int k = 0; k < n; k++) acc += Sinv[(size_t)k * n + r] * A[h * nn + (size_t)col * n + k];
+                Aout[h * nn + (size_t)col * n + r] = acc;
+                s2 += acc * acc;
+            }
+            const double nr = sqrt(s2);
+            for (int r = 0; r < n; r++) Aout[h * nn + (size_t)col * n + r] /= nr;
+        }
+    }
+    std::vector<double> ll;
+    for (const auto& r : c->hist) ll.push_back(r.ll);
+    if (p->weightsfile) TRY(write_doubles(p->weightsfile, W.data(), W.size()));
+    if (p->afile) TRY(write_doubles(p->afile, Aout.data(), Aout.size()));
+    if (p->cfile) TRY(write_doubles(p->cfile, cout_.data(), cout_.size()));
+    if (p->gmfile) TRY(write_doubles(p->gmfile, gm.data(), gm.size()));
+    if (p->alphafile) TRY(write_doubles(p->alphafile, alpha.data(), alpha.size()));
+    if (p->betafile) TRY(write_doubles(p->betafile, beta.data(), beta.size()));
+    if (p->mufile) TRY(write_doubles(p->mufile, mu.data(), mu.size()));
+    if (p->rhofile) TRY(write_doubles(p->rhofile, rho.data(), rho.size()));
+    if (p->llfile) TRY(write_doubles(p->llfile, ll.data(), ll.size()));
+    if (p->spherefile) TRY(write_doubles(p->spherefile, S.data(), S.size()));
+    if (p->ltallfile && c->have_estep) {
+        std::vector<double> Lt((size_t)M * c->T);
+        TRY(amica_get_loglik(c, Lt.data(), nullptr, nullptr));
+        TRY(write_doubles(p->ltallfile, Lt.data(), Lt.size()));
+    }
+    return AMICA_OK;
+}
+
+int amica_last_cuda_error(void) { return g_last_cuda_error; }
+
+int64_t amica_launches_per_iteration(amica_ctx* c) { return c ? launches_per_iteration(c) : 0; }
+
+int amica_set_iter_state(amica_ctx* c, int64_t iter, double lrate, double ll_prev) {
+    if (!c || iter < 0 || !(lrate > 0.0)) return AMICA_ERR_INVALIDPARAM;
+    if (!c->have_init) return AMICA_ERR_STATE;
+    CK(cudaSetDevice(c->dev));
+    CK(cudaMemcpyAsync(c->h_ctrl, c->b.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->h_ctrl->iter = iter;
+    c->h_ctrl->lrate = lrate;
+    c->h_ctrl->ll_prev = ll_prev;
+    CK(cudaMemcpyAsync(c->b.ctrl, c->h_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return AMICA_OK;
+}
+
+int amica_time_estep(amica_ctx* c, int64_t reps, double* ms_per_launch, int64_t* launches) {
+    if (!c || reps < 1 || !ms_per_launch) return AMICA_ERR_INVALIDPARAM;
+    if (!c->have_x || !c->have_init) return AMICA_ERR_STATE;
+    CK(cudaSetDevice(c->dev));
+    CK(launch_prep(c->b, c->hc, c->st));
+    EStepArgs a = estep_args(c);
+    // one untimed launch, then reps timed back-to-back launches of the fused kernel
+    if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st));
+    else CK(launch_estep_plain(a, c->NP, c->nclusters, c->st));
+    CK(cudaEventRecord(c->ev0, c->st));
+    for (int64_t r = 0; r < reps; r++) {
+        if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st));
+        else CK(launch_estep_plain(a, c->NP, c->nclusters, c->st));
+    }
+    CK(cudaEventRecord(c->ev1, c->st));
+    CK(cudaEventSynchronize(c->ev1));
+    TRY(check_device_error(c));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    *ms_per_launch = (double)ms / (double)reps;
+    if (launches) *launches = reps + 2;
+    return AMICA_OK;
+}
+
+int amica_get_sphere(amica_ctx* c, double* sphere, double* means, double* ldetS) {
+    if (!c) return AMICA_ERR_INVALIDPARAM;
+    if (!c->have_x) return AMICA_ERR_STATE;
+    CK(cudaSetDevice(c->dev));
+    CK(cudaStreamSynchronize(c->st));
+    if (sphere) CK(cudaMemcpy(sphere, c->d_sphere, sizeof(double) * c->n * c->n, cudaMemcpyDeviceToHost));
+    if (means) CK(cudaMemcpy(means, c->d_means, sizeof(double) * c->n, cudaMemcpyDeviceToHost));
+    if (ldetS) *ldetS = c->ldetS;
+    return AMICA_OK;
+}
+
+}  // extern "C"

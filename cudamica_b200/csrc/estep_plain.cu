@@ -41,8 +41,9 @@ struct PlainShape {
     // Psi update: each thread RI x RK block
     static constexpr int RI = NP / 16;
     static constexpr int RK = NP / 16;
+    static constexpr int LLD = NP + 1;              // padded row of the lse tile
     static constexpr size_t smem_floats =
-        (size_t)NP * WLD + (size_t)kS * XLD + (size_t)kS * NP * 2 + 2 * kS + 2 * kS;
+        (size_t)NP * WLD + (size_t)kS * XLD + (size_t)kS * NP + (size_t)kS * LLD + 2 * kS + 2 * kS;
 };
 
 template <int NP, int MM>
@@ -52,10 +53,9 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     float* Wt = sm;                                   // [NP][WLD]  Wt[k][i] = W[i][k]
     float* xs = Wt + NP * Sh::WLD;                    // [S][XLD]
     float* bs = xs + kS * Sh::XLD;                    // [S][NP]    (W x)_i per sample
-    float* gs = bs + kS * NP;                         // [S][NP]    g, aliased with lse
-    float* slot = gs + kS * NP;                       // [2][S]     cluster-visible L_h(t)
+    float* gs = bs + kS * NP;                         // [S][NP] g; as lse: [S][LLD]
+    float* slot = gs + kS * Sh::LLD;                  // [2][S]     cluster-visible L_h(t)
     float* vS = slot + 2 * kS;                        // [S]        v_h(t) (0 if not used)
-    float* spare = vS + kS;                           // [S]
 
     cg::cluster_group cluster = cg::this_cluster();
     const int h = (int)cluster.block_rank();
@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     const float wci = a.wc[(size_t)h * NP + ch];
     float ltc[kMaxModels];
 #pragma unroll
-    for (int q = 0; q < kMaxModels; q++) ltc[q] = (q < M) ? a.ltcrel[q] : 0.f;
+    for (int q = 0; q < kMaxModels; q++) ltc[q] = (q < M) ? (float)(a.ltc64[q] - a.ltc64[0]) : 0.f;
 
     // FP64 running sums for this thread's channel
     double dUs[MM], dKn[MM], dLn[MM], dMn[MM], dMd[MM], dBd[MM], dRn[MM];
@@ -160,14 +160,14 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
             float se = 0.f;
 #pragma unroll
             for (int j = 0; j < MM; j++) se += ptx_ex2(q[j] - qmax);
-            lse[t * NP + ch] = ch_ok ? qmax + ptx_lg2(se) : 0.f;
+            lse[t * Sh::LLD + ch] = ch_ok ? qmax + ptx_lg2(se) : 0.f;
         }
         __syncthreads();
         // ---- Lt_h(t): channel sum in fixed order, published for the cluster
         float* myslot = slot + par * kS;
         if (tid < kS) {
             float s = 0.f;
-            for (int i = 0; i < n; i++) s += lse[tid * NP + i];
+            for (int i = 0; i < n; i++) s += lse[tid * Sh::LLD + i];
             myslot[tid] = ltc[h] + kLn2 * s;
         }
         cluster.sync();
@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
                     const float lv = fmaf(fp, y[j], -1.f);
                     fLn[j] = fmaf(u * lv, lv, fLn[j]);
                     fMn[j] += ufp;
-                    if (pr[j] <= 2.f) {
+                    if (pr[j] <= 2.f || a.grad_mode) {
                         fMd[j] = fmaf(ufp, copysignf(ri, y[j]), fMd[j]);
                         fBd[j] = fmaf(ufp, y[j], fBd[j]);
                     } else {
@@ -290,38 +290,32 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     // ---- write this CTA's partial sums (fixed-order combination of groups)
     PartLayout L{n, MM};
     double* out = a.partial + ((size_t)cid * M + h) * L.stride();
-    double* red = reinterpret_cast<double*>(xs);   // reuse x/b/g tiles: [SPLIT][24?][NP]
+    double* red = reinterpret_cast<double*>(xs);   // [SPLIT][NP] doubles, one statistic at a time
     constexpr int NACC = 7 * MM + 3;
-    {
-        double vals[NACC];
+    double vals[NACC];
 #pragma unroll
-        for (int j = 0; j < MM; j++) {
-            vals[0 * MM + j] = dUs[j]; vals[1 * MM + j] = dKn[j]; vals[2 * MM + j] = dLn[j];
-            vals[3 * MM + j] = dMn[j]; vals[4 * MM + j] = dMd[j]; vals[5 * MM + j] = dBd[j];
-            vals[6 * MM + j] = dRn[j];
-        }
-        vals[7 * MM + 0] = dCn; vals[7 * MM + 1] = dS2; vals[7 * MM + 2] = dGs;
+    for (int j = 0; j < MM; j++) {
+        vals[0 * MM + j] = dUs[j]; vals[1 * MM + j] = dKn[j]; vals[2 * MM + j] = dLn[j];
+        vals[3 * MM + j] = dMn[j]; vals[4 * MM + j] = dMd[j]; vals[5 * MM + j] = dBd[j];
+        vals[6 * MM + j] = dRn[j];
+    }
+    vals[7 * MM + 0] = dCn; vals[7 * MM + 1] = dS2; vals[7 * MM + 2] = dGs;
 #pragma unroll
-        for (int k = 0; k < NACC; k++) red[((size_t)grp * NACC + k) * NP + ch] = vals[k];
-    }
-    __syncthreads();
-    for (int e = tid; e < NACC * NP; e += kThreads) {
-        const int k = e / NP, i = e % NP;
-        if (i >= n) continue;
-        double s = 0.0;
-        for (int g2 = 0; g2 < Sh::SPLIT; g2++) s += red[((size_t)g2 * NACC + k) * NP + i];
-        if (k < 7 * MM) {
-            const int stat = k / MM, j = k % MM;
-            out[L.mix(stat) + j * n + i] = s;
-        } else if (k == 7 * MM) {
-            out[L.cn() + i] = s;
-        } else if (k == 7 * MM + 1) {
-            out[L.s2() + i] = s;
-        } else {
-            out[L.gs() + i] = s;
+    for (int k = 0; k < NACC; k++) {
+        red[grp * NP + ch] = vals[k];
+        __syncthreads();
+        if (tid < NP && tid < n) {
+            double s = 0.0;
+            for (int g2 = 0; g2 < Sh::SPLIT; g2++) s += red[g2 * NP + tid];
+            int dst;
+            if (k < 7 * MM) dst = L.mix(k / MM) + (k % MM) * n + tid;
+            else if (k == 7 * MM) dst = L.cn() + tid;
+            else if (k == 7 * MM + 1) dst = L.s2() + tid;
+            else dst = L.gs() + tid;
+            out[dst] = s;
         }
+        __syncthreads();
     }
-    __syncthreads();
     // LL numerator and vsum: per-sample threads, combined in fixed order
     double* red2 = red;
     if (tid < kS) { red2[tid] = dLL; red2[kS + tid] = dVs; }
@@ -381,22 +375,48 @@ int plain_tile_samples() { return kS; }
 
 int plain_pad_channels(int n) { return n <= 32 ? 32 : (n <= 64 ? 64 : (n <= 128 ? 128 : -1)); }
 
-// Largest cluster count whose clusters can all be resident at once.
+// Largest cluster count whose clusters can all be resident at once (the grid
+// is persistent: every cluster loops over its share of the tiles).
+template <int NP, int MM>
+int max_active_clusters(int M) {
+    using Sh = PlainShape<NP>;
+    const size_t smem = Sh::smem_floats * sizeof(float);
+    auto kern = estep_plain_kernel<NP, MM>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return -1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(M * 64);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = M;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int num = 0;
+    if (cudaOccupancyMaxActiveClusters(&num, kern, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    return num;
+}
+
 int plain_max_clusters(int n, int m, int M) {
-    int NP = plain_pad_channels(n);
+    const int NP = plain_pad_channels(n);
     if (NP < 0 || m < 1 || m > 5 || M < 1 || M > kMaxModels) return -1;
-    size_t smem = 0;
-    if (NP == 32) smem = PlainShape<32>::smem_floats * 4;
-    if (NP == 64) smem = PlainShape<64>::smem_floats * 4;
-    if (NP == 128) smem = PlainShape<128>::smem_floats * 4;
-    int dev = 0, sms = 0, maxsmem = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-    int per_sm = (int)(maxsmem / (smem + 1024));
-    if (per_sm < 1) return -1;
-    int ctas = sms * per_sm;
-    return ctas / M;
+#define AMICA_PLAIN_OCC(NPV, MMV) \
+    if (NP == NPV && m == MMV) return max_active_clusters<NPV, MMV>(M);
+#define AMICA_PLAIN_OCC_NP(NPV) \
+    AMICA_PLAIN_OCC(NPV, 1) AMICA_PLAIN_OCC(NPV, 2) AMICA_PLAIN_OCC(NPV, 3) \
+    AMICA_PLAIN_OCC(NPV, 4) AMICA_PLAIN_OCC(NPV, 5)
+    AMICA_PLAIN_OCC_NP(32)
+    AMICA_PLAIN_OCC_NP(64)
+    AMICA_PLAIN_OCC_NP(128)
+#undef AMICA_PLAIN_OCC_NP
+#undef AMICA_PLAIN_OCC
+    return -1;
 }
 
 cudaError_t launch_estep_plain(const EStepArgs& a, int NP, int nclusters, cudaStream_t st) {

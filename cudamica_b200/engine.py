@@ -1,0 +1,274 @@
+"""Python mirror of the engine's C ABI (include/amica_b200.h), over ctypes.
+
+The reference has no Python or library API -- its EM loop is
+``runamica()`` behind the ``cudaamica -f <params>`` executable
+(src/cudaamica.cu:17-43, src/amica.cu:624) -- so this module mirrors the C ABI
+one to one.  It needs the in-tree shared library built for sm_100a
+(``python -m cudamica_b200.build``) and raises if it is missing: there is no
+CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libamica_b200.so")
+
+AMICA_PREC_FP32 = 0
+AMICA_PREC_MIXED = 1
+
+_i64 = C.c_int64
+_dbl = C.c_double
+_pd = C.POINTER(C.c_double)
+_pf = C.POINTER(C.c_float)
+_pu8 = C.POINTER(C.c_uint8)
+
+CFG_INT_FIELDS = (
+    "nchannels", "nsamples", "nmmodels", "nsdm", "maxiter", "do_sphere", "block_size", "fix_init",
+    "do_newton", "update_rho", "rho_start_iter", "newt_start_iter", "maxdec", "update_gm",
+    "update_alpha", "update_A", "update_mu", "update_beta", "do_reparm", "do_reject", "rejstart",
+    "rejint", "maxrej", "precision", "device", "seed", "verbose")
+CFG_DBL_FIELDS = ("lrate0", "lratemax", "lnatrate", "lratefact", "rho0", "rholrate", "rhomin",
+                  "rhomax", "rejsig")
+
+EXPORTED = (
+    "amica_default_cfg", "amica_create", "amica_destroy", "amica_load_data",
+    "amica_load_data_device", "amica_preprocess", "amica_set_sphered", "amica_init",
+    "amica_em_step", "amica_run", "amica_get_params", "amica_set_params", "amica_estep_stats",
+    "amica_stats_len", "amica_get_loglik", "amica_loglik_adjoint", "amica_reject_now",
+    "amica_write_outputs", "amica_status_string", "amica_kernel_name", "amica_get_p_relative",
+    "amica_last_cuda_error", "amica_set_iter_state", "amica_get_sphere", "amica_time_estep",
+    "amica_launches_per_iteration")
+
+
+class Cfg(C.Structure):
+    _fields_ = [(k, _i64) for k in CFG_INT_FIELDS] + [(k, _dbl) for k in CFG_DBL_FIELDS]
+
+
+class IterOut(C.Structure):
+    _fields_ = [("iter", _i64), ("ll", _dbl), ("lrate", _dbl), ("ll_decreased", _i64),
+                ("newton", _i64), ("nkeep", _i64), ("nrejected", _i64), ("device_ms", _dbl)]
+
+
+class Paths(C.Structure):
+    _fields_ = [(k, C.c_char_p) for k in (
+        "weightsfile", "afile", "cfile", "ltallfile", "gmfile", "alphafile", "mufile",
+        "betafile", "rhofile", "llfile", "spherefile")]
+
+
+class AmicaError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        self.code = code
+        msg = lib().amica_status_string(code).decode()
+        super().__init__(f"{where}: status {code} ({msg})")
+
+
+_lib = None
+
+
+def lib():
+    """Load libamica_b200.so; raise if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with python -m cudamica_b200.build")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.amica_default_cfg.argtypes = [C.POINTER(Cfg)]
+        L.amica_create.argtypes = [C.POINTER(Cfg), C.POINTER(vp)]
+        L.amica_destroy.argtypes = [vp]
+        L.amica_load_data.argtypes = [vp, _pf, _i64, _i64]
+        L.amica_load_data_device.argtypes = [vp, vp, _i64, _i64]
+        L.amica_preprocess.argtypes = [vp]
+        L.amica_set_sphered.argtypes = [vp, _pd, _pd, _pd, _dbl]
+        L.amica_init.argtypes = [vp, _pd, _pd]
+        L.amica_em_step.argtypes = [vp, C.POINTER(IterOut)]
+        L.amica_run.argtypes = [vp, _i64, C.POINTER(IterOut)]
+        L.amica_get_params.argtypes = [vp] + [_pd] * 8
+        L.amica_set_params.argtypes = [vp] + [_pd] * 7
+        L.amica_estep_stats.argtypes = [vp, _pd]
+        L.amica_stats_len.restype = _i64
+        L.amica_stats_len.argtypes = [_i64, _i64, _i64]
+        L.amica_get_loglik.argtypes = [vp, _pd, _pd, _pu8]
+        L.amica_loglik_adjoint.argtypes = [vp, _pd, _pd, _pd, _pd, _pd]
+        L.amica_reject_now.argtypes = [vp, C.POINTER(_i64)]
+        L.amica_write_outputs.argtypes = [vp, C.POINTER(Paths)]
+        L.amica_status_string.restype = C.c_char_p
+        L.amica_status_string.argtypes = [C.c_int]
+        L.amica_kernel_name.restype = C.c_char_p
+        L.amica_kernel_name.argtypes = [vp]
+        L.amica_get_p_relative.argtypes = [vp, _pf]
+        L.amica_set_iter_state.argtypes = [vp, _i64, _dbl, _dbl]
+        L.amica_get_sphere.argtypes = [vp, _pd, _pd, _pd]
+        L.amica_time_estep.argtypes = [vp, _i64, _pd, C.POINTER(_i64)]
+        L.amica_launches_per_iteration.restype = _i64
+        L.amica_launches_per_iteration.argtypes = [vp]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_pd)
+
+
+def _chk(rc: int, where: str) -> None:
+    if rc != 0:
+        raise AmicaError(rc, where)
+
+
+def default_cfg(**over) -> Cfg:
+    c = Cfg()
+    _chk(lib().amica_default_cfg(C.byref(c)), "amica_default_cfg")
+    for k, v in over.items():
+        setattr(c, k, v)
+    return c
+
+
+class Amica:
+    """One fit on one GPU: a thin owner of an amica_ctx."""
+
+    def __init__(self, n: int, T: int, M: int = 1, m: int = 3, **cfg_over):
+        self.cfg = default_cfg(nchannels=n, nsamples=T, nmmodels=M, nsdm=m, **cfg_over)
+        self.n, self.T, self.M, self.m = n, T, M, m
+        self._ctx = C.c_void_p()
+        _chk(lib().amica_create(C.byref(self.cfg), C.byref(self._ctx)), "amica_create")
+
+    # -- lifecycle -------------------------------------------------------
+    def close(self) -> None:
+        if self._ctx:
+            lib().amica_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def kernel(self) -> str:
+        return lib().amica_kernel_name(self._ctx).decode()
+
+    # -- data --------------------------------------------------------------
+    def load_data(self, x: np.ndarray) -> None:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        assert x.shape == (self.T, self.n)
+        _chk(lib().amica_load_data(self._ctx, x.ctypes.data_as(_pf), self.n, self.T),
+             "amica_load_data")
+
+    def load_data_device(self, ptr: int) -> None:
+        _chk(lib().amica_load_data_device(self._ctx, C.c_void_p(ptr), self.n, self.T),
+             "amica_load_data_device")
+
+    def preprocess(self) -> None:
+        _chk(lib().amica_preprocess(self._ctx), "amica_preprocess")
+
+    def set_sphered(self, xs, means=None, sphere=None, ldetS: float = 0.0) -> None:
+        xs = np.ascontiguousarray(xs, dtype=np.float64)
+        mn = None if means is None else np.ascontiguousarray(means, dtype=np.float64)
+        sp = None if sphere is None else np.ascontiguousarray(np.asarray(sphere).T, dtype=np.float64)
+        _chk(lib().amica_set_sphered(self._ctx, _p(xs), _p(mn), _p(sp), float(ldetS)),
+             "amica_set_sphered")
+
+    def init(self, A0=None, c0=None) -> None:
+        a = None if A0 is None else np.ascontiguousarray(A0, dtype=np.float64)
+        c = None if c0 is None else np.ascontiguousarray(c0, dtype=np.float64)
+        _chk(lib().amica_init(self._ctx, _p(a), _p(c)), "amica_init")
+
+    # -- iterations --------------------------------------------------------
+    def step(self) -> IterOut:
+        out = IterOut()
+        _chk(lib().amica_em_step(self._ctx, C.byref(out)), "amica_em_step")
+        return out
+
+    def run(self, iters: int) -> list:
+        outs = (IterOut * max(iters, 1))()
+        _chk(lib().amica_run(self._ctx, iters, outs), "amica_run")
+        return [outs[k] for k in range(iters)]
+
+    # -- state -------------------------------------------------------------
+    def params(self) -> dict:
+        n, M, m = self.n, self.M, self.m
+        out = dict(A=np.empty((M, n, n)), W=np.empty((M, n, n)), c=np.empty((M, n)),
+                   gm=np.empty(M), alpha=np.empty((M, m, n)), mu=np.empty((M, m, n)),
+                   beta=np.empty((M, m, n)), rho=np.empty((M, m, n)))
+        _chk(lib().amica_get_params(self._ctx, *[_p(out[k]) for k in
+                                                 ("A", "W", "c", "gm", "alpha", "mu", "beta",
+                                                  "rho")]), "amica_get_params")
+        return out
+
+    def set_params(self, **kw) -> None:
+        args = []
+        for k in ("A", "c", "gm", "alpha", "mu", "beta", "rho"):
+            v = kw.get(k)
+            args.append(None if v is None else np.ascontiguousarray(v, dtype=np.float64))
+        self._keep = args
+        _chk(lib().amica_set_params(self._ctx, *[_p(a) for a in args]), "amica_set_params")
+
+    def estep_stats(self) -> np.ndarray:
+        L = lib().amica_stats_len(self.n, self.M, self.m)
+        s = np.empty(L)
+        _chk(lib().amica_estep_stats(self._ctx, _p(s)), "amica_estep_stats")
+        return s
+
+    def loglik(self):
+        Lt = np.empty((self.M, self.T))
+        P = np.empty(self.T)
+        keep = np.empty(self.T, dtype=np.uint8)
+        _chk(lib().amica_get_loglik(self._ctx, _p(Lt), _p(P), keep.ctypes.data_as(_pu8)),
+             "amica_get_loglik")
+        return Lt, P, keep
+
+    def p_relative(self) -> np.ndarray:
+        P = np.empty(self.T, dtype=np.float32)
+        _chk(lib().amica_get_p_relative(self._ctx, P.ctypes.data_as(_pf)), "amica_get_p_relative")
+        return P
+
+    def set_iter_state(self, iter: int, lrate: float, ll_prev: float) -> None:
+        _chk(lib().amica_set_iter_state(self._ctx, iter, lrate, ll_prev), "amica_set_iter_state")
+
+    def sphere(self):
+        S = np.empty((self.n, self.n))
+        means = np.empty(self.n)
+        ld = np.empty(1)
+        _chk(lib().amica_get_sphere(self._ctx, _p(S), _p(means), _p(ld)), "amica_get_sphere")
+        return S.T.copy(), means, float(ld[0])
+
+    def time_estep(self, reps: int = 10):
+        ms = np.empty(1)
+        nl = _i64()
+        _chk(lib().amica_time_estep(self._ctx, reps, _p(ms), C.byref(nl)), "amica_time_estep")
+        return float(ms[0]), int(nl.value)
+
+    @property
+    def launches_per_iteration(self) -> int:
+        return int(lib().amica_launches_per_iteration(self._ctx))
+
+    def reject_now(self) -> int:
+        k = _i64()
+        _chk(lib().amica_reject_now(self._ctx, C.byref(k)), "amica_reject_now")
+        return int(k.value)
+
+    def adjoint(self):
+        n, M, m = self.n, self.M, self.m
+        ll = np.empty(1)
+        dW = np.empty((M, n, n))
+        dmu = np.empty((M, m, n))
+        dbeta = np.empty((M, m, n))
+        drho = np.empty((M, m, n))
+        _chk(lib().amica_loglik_adjoint(self._ctx, _p(ll), _p(dW), _p(dmu), _p(dbeta), _p(drho)),
+             "amica_loglik_adjoint")
+        return float(ll[0]), dict(W=dW, mu=dmu, beta=dbeta, rho=drho)
+
+    def write_outputs(self, **paths) -> None:
+        p = Paths(**{k: (v.encode() if v else None) for k, v in paths.items()})
+        _chk(lib().amica_write_outputs(self._ctx, C.byref(p)), "amica_write_outputs")

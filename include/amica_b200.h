@@ -161,6 +161,29 @@ typedef struct amica_paths {
 } amica_paths;
 int amica_write_outputs(amica_ctx *ctx, const amica_paths *paths);
 
+/* P(t) minus log gm_0 + ldet_0 + ldetS, as float, exactly as the kernels
+ * stored it (the input of the rejection rule). */
+int amica_get_p_relative(amica_ctx *ctx, float *P);
+
+/* Resume support: set the iteration counter, learning rate and previous LL
+ * (the host-side loop state of src/amica.cu:800-806) after amica_init() +
+ * amica_set_params(), so a fit can continue from saved parameters. */
+int amica_set_iter_state(amica_ctx *ctx, int64_t iter, double lrate, double ll_prev);
+
+/* Sphering matrix (n x n, column-major), channel means and ldetS in use. */
+int amica_get_sphere(amica_ctx *ctx, double *sphere, double *means, double *ldetS);
+
+/* Time the fused E-step kernel alone on the context's stream with CUDA
+ * events: reps back-to-back launches after one warm launch.  *launches gets
+ * the number of kernels launched (may be NULL). */
+int amica_time_estep(amica_ctx *ctx, int64_t reps, double *ms_per_launch, int64_t *launches);
+
+/* Number of kernels one EM iteration launches. */
+int64_t amica_launches_per_iteration(amica_ctx *ctx);
+
+/* Last CUDA runtime error code seen by any call (0 = none). */
+int amica_last_cuda_error(void);
+
 /* Message for a status code (replaces cGetErrorString, src/error.cu:14-16). */
 const char *amica_status_string(int status);
 

@@ -1,0 +1,165 @@
+"""GPU parity tests: the CUDA engine (through its C ABI) against the FP64 oracle
+and the reference's own golden trajectories.
+
+Tolerances (FP32 densities, FP32 per-tile sums, FP64 totals):
+  * E-step statistics at identical parameters: relative error <= 2e-5 for the
+    well-conditioned sums (usum, vsum, cnew, sigma2, kappa, lambda, mu_num,
+    beta_den, rho_num, phi) and <= 3e-2 for mu_den, whose terms
+    u rho |y|^(rho-2) are heavy-tailed near y = 0: the sample nearest y = 0
+    carries up to ~5% of the sum at these sizes, so rounding y to FP32 alone
+    (absolute error ~1e-7) moves the sum by up to ~1% (measured on c0 with
+    numpy).  The same sum makes two FP64 implementations drift apart over
+    iterations.
+  * LL per sample and channel: <= 2e-6 at identical parameters; along a
+    trajectory the difference grows by the factor the FP64 oracle-vs-reference
+    comparison shows (x5 per iteration allowed here).
+"""
+import numpy as np
+import pytest
+
+from golden.cases import CASES, prepared
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+STAT_KEYS_TIGHT = ("vs", "cn", "s2", "us", "kn", "ln", "mn", "bd", "rn", "phi")
+
+
+def _engine(case, p, precision=0, ldetS=None, **over):
+    from cudamica_b200.engine import Amica
+    eng = Amica(case.n, case.T, case.M, case.m, precision=precision,
+                newt_start_iter=case.newt_start_iter, update_rho=int(case.update_rho), **over)
+    eng.set_sphered(p["xs"], p["means"], p["sphere"], p["ldetS"] if ldetS is None else ldetS)
+    eng.init(p["A0"], p["c0"])
+    return eng
+
+
+def _oracle(case, p, ldetS=None):
+    return O.Oracle(p["xs"], case.M, case.m, p["A0"], p["c0"],
+                    p["ldetS"] if ldetS is None else ldetS, nthreads=8,
+                    newt_start_iter=case.newt_start_iter, update_rho=int(case.update_rho))
+
+
+def _compare_stats(s_gpu, s_orc, n, M, m, tight=2e-5, md_tol=3e-2):
+    a = O.split_stats(s_gpu, n, M, m)
+    b = O.split_stats(s_orc, n, M, m)
+    errs = {}
+    vsum = float(np.max(b["vs"]))
+    for k in STAT_KEYS_TIGHT + ("md",):
+        scale = np.max(np.abs(b[k]))
+        if k == "cn":   # sums of centred data are ~0: measure against sum v |x| ~ vsum
+            scale = max(scale, vsum)
+        errs[k] = float(np.max(np.abs(a[k] - b[k])) / max(scale, 1e-300))
+    for k in STAT_KEYS_TIGHT:
+        assert errs[k] < tight, (k, errs)
+    assert errs["md"] < md_tol, errs
+    return errs
+
+
+@pytest.fixture(scope="module")
+def preps():
+    return {k: prepared(CASES[k]) for k in CASES}
+
+
+@pytest.mark.parametrize("name", ["c0", "m2", "m3"])
+@pytest.mark.parametrize("precision", [0])
+def test_estep_stats_match_oracle(name, precision, preps):
+    case, p = CASES[name], preps[name]
+    eng = _engine(case, p, precision)
+    orc = _oracle(case, p)
+    # at the initial state and after 3 oracle iterations (different A, mu, beta, rho)
+    for it in range(2):
+        if it == 1:
+            for _ in range(3):
+                orc.step()
+            eng.set_params(A=orc.A, c=orc.c, gm=orc.gm, alpha=orc.alpha, mu=orc.mu,
+                           beta=orc.beta, rho=orc.rho)
+        orc.prepare()
+        s_orc = orc.estep()
+        s_gpu = eng.estep_stats()
+        n_ll = case.n * case.T
+        assert abs(s_gpu[0] - s_orc[0]) / n_ll < 2e-6
+        _compare_stats(s_gpu, s_orc, case.n, case.M, case.m)
+    eng.close()
+
+
+@pytest.mark.parametrize("name,iters", [("c0", 5), ("m2", 3), ("m3", 3)])
+def test_first_iterations_vs_reference(name, iters, preps):
+    case, p = CASES[name], preps[name]
+    ref = np.load(f"{pytest.golden_dir}/ref_{name}.npz")
+    eng = _engine(case, p, 0, ldetS=float(ref["ldetS"][0]))
+    for it in range(1, iters + 1):
+        out = eng.step()
+        assert out.iter == it
+        assert abs(out.lrate - ref["lrate"][it - 1]) < 1e-15
+        assert abs(out.ll - ref["ll"][it - 1]) < 2e-6 * 5 ** (it - 1), (it, out.ll, ref["ll"][it - 1])
+    keep = list(ref["keep_iters"])
+    prm = eng.params()
+    if iters in keep:
+        a = keep.index(iters)
+        A_ref = ref["iter_A"][a]
+        assert np.max(np.abs(prm["A"] - A_ref)) / np.max(np.abs(A_ref)) < 1e-3
+    eng.close()
+
+
+@pytest.mark.parametrize("k", [1, 50, 51])
+def test_one_step_from_reference_state(k, preps):
+    case, p = CASES["c0"], preps["c0"]
+    ref = np.load(f"{pytest.golden_dir}/ref_c0.npz")
+    keep = list(ref["keep_iters"])
+    a, b = keep.index(k), keep.index(k + 1)
+    eng = _engine(case, p, 0, ldetS=float(ref["ldetS"][0]))
+    eng.set_params(A=ref["iter_A"][a], c=ref["iter_c"][a], alpha=ref["iter_alpha"][a],
+                   mu=ref["iter_mu"][a], beta=ref["iter_beta"][a], rho=ref["iter_rho"][a])
+    orc = _oracle(case, p, ldetS=float(ref["ldetS"][0]))
+    for key in ("A", "c", "alpha", "mu", "beta", "rho"):
+        getattr(orc, key)[...] = ref["iter_" + key][a]
+    # same control state as the reference had entering iteration k+1
+    orc.st.iter = k
+    orc.st.lrate = float(ref["lrate"][k])
+    orc.st.ll_prev = float(ref["ll"][k - 1])
+    eng.set_iter_state(k, float(ref["lrate"][k]), float(ref["ll"][k - 1]))
+    out = eng.step()
+    orc.step()
+    assert abs(out.ll - ref["ll"][k]) < 2e-6
+    prm = eng.params()
+    for key in ("A", "alpha", "beta", "rho"):
+        r = ref["iter_" + key][b]
+        err = np.max(np.abs(prm[key] - r)) / np.max(np.abs(r))
+        assert err < 2e-4, (key, err)
+    eng.close()
+
+
+def test_run_graph_matches_steps(preps):
+    case, p = CASES["m2"], preps["m2"]
+    e1 = _engine(case, p, 0)
+    e2 = _engine(case, p, 0)
+    outs1 = [e1.step() for _ in range(6)]
+    outs2 = e2.run(6)
+    for a, b in zip(outs1, outs2):
+        assert a.ll == b.ll and a.lrate == b.lrate
+    p1, p2 = e1.params(), e2.params()
+    for k in p1:
+        assert np.array_equal(p1[k], p2[k]), k
+    e1.close()
+    e2.close()
+
+
+def test_gpu_preprocess_matches_numpy(preps):
+    case, p = CASES["c0"], preps["c0"]
+    from cudamica_b200.engine import Amica
+    eng = Amica(case.n, case.T, case.M, case.m, precision=0)
+    eng.load_data(p["x"])
+    eng.preprocess()
+    eng.init(p["A0"], p["c0"])
+    S, means, ld = eng.sphere()
+    assert np.max(np.abs(S - p["sphere"])) < 1e-10
+    assert np.max(np.abs(means - p["means"])) < 1e-12
+    assert abs(ld - p["ldetS"]) < 1e-10
+    eng_ref = _engine(case, p, 0)
+    s1 = eng.estep_stats()
+    s2 = eng_ref.estep_stats()
+    # same whitened data up to FP32 rounding: LL numerators agree closely
+    assert abs(s1[0] - s2[0]) / (case.n * case.T) < 1e-6
+    eng.close()
+    eng_ref.close()
