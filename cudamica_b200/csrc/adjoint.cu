@@ -56,7 +56,7 @@ __global__ void k_adjoint_reduce(const double* __restrict__ partial, double* __r
 __global__ void k_adjoint_finalize(const double* __restrict__ raw, const double* __restrict__ A,
                                    const double* __restrict__ c, const double* __restrict__ beta,
                                    const double* __restrict__ rho, double* __restrict__ out, int n,
-                                   int m, int M) {
+                                   int m, int M, int psi_is_phi) {
     const int h = blockIdx.x;
     PartLayout PL{n, m};
     const double* R = raw + (size_t)h * PL.stride();
@@ -68,8 +68,15 @@ __global__ void k_adjoint_finalize(const double* __restrict__ raw, const double*
     const double* gs = R + PL.gs();
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
         const int i = e % n, k = e / n;   // dW(i,k) stored at k*n + i
-        // W^{-T}(i,k) = A(k,i)
-        dW[e] = vsum * Ah[(size_t)i * n + k] - (Psi[(size_t)k * n + i] - gs[i] * c[(size_t)h * n + k]);
+        // W^{-T}(i,k) = A(k,i); sum_t g (x - c)^T = Psi - gsum c^T = phi W^{-T} = phi A^T
+        double gx;
+        if (psi_is_phi) {
+            gx = 0.0;
+            for (int l = 0; l < n; l++) gx += Psi[(size_t)l * n + i] * Ah[(size_t)l * n + k];
+        } else {
+            gx = Psi[(size_t)k * n + i] - gs[i] * c[(size_t)h * n + k];
+        }
+        dW[e] = vsum * Ah[(size_t)i * n + k] - gx;
     }
     const size_t off_mu = 1 + (size_t)M * n * n;
     const size_t mnM = (size_t)M * m * n;
@@ -100,13 +107,13 @@ cudaError_t launch_adjoint(const EStepArgs& a0, int NP, double* grad_partial, in
 cudaError_t launch_adjoint_finalize(const double* grad_partial, double* raw, int nclusters, int n,
                                     int m, int M, const double* A, const double* c,
                                     const double* beta, const double* rho, double* out,
-                                    cudaStream_t st) {
+                                    int psi_is_phi, cudaStream_t st) {
     PartLayout PL{n, m};
     const int64_t total = (int64_t)M * PL.stride();
     int grid = (int)((total + 255) / 256);
     if (grid > 4096) grid = 4096;
     k_adjoint_reduce<<<grid, 256, 0, st>>>(grad_partial, raw, nclusters, M, PL.stride());
-    k_adjoint_finalize<<<M, 256, 0, st>>>(raw, A, c, beta, rho, out, n, m, M);
+    k_adjoint_finalize<<<M, 256, 0, st>>>(raw, A, c, beta, rho, out, n, m, M, psi_is_phi);
     return cudaGetLastError();
 }
 

@@ -41,10 +41,13 @@ struct IterRec {
     int64_t iter, newton, ll_decreased, nkeep, nrejected, pad;
 };
 
-// Layout of one CTA's partial sums (doubles), model h of a cluster:
-//   [0] LL numerator (rank 0 only), [1] vsum, then per channel cn, s2, gsum
-//   (n each), then usum, kn, ln, mn, md, bd, rn (m*n each, mixture-major),
-//   then Psi = sum_t g x^T (n*n, column-major: Psi(i,k) at k*n + i).
+// Layout of one partial-sum slot (doubles), model h:
+//   [0] LL numerator (model 0 only), [1] vsum, then per channel
+//   sum v b (n; b = W(x - c), from which cnew = A sum(v b) / vsum + c),
+//   s2 = sum v b^2 (n), gsum = sum g (n), then usum, kn, ln, mn, md, bd, rn
+//   (m*n each, mixture-major), then the n*n contraction (column-major, (i,k)
+//   at k*n + i): Psi = sum_t g x^T from the plain kernel, or phi = sum_t g b^T
+//   from the tensor-core kernel.  Slots are summed in a fixed order by k_reduce.
 struct PartLayout {
     int n, m;
     __host__ __device__ int cn() const { return 2; }
@@ -109,6 +112,7 @@ struct MStepCfgHost {
     int update_gm, update_alpha, update_A, update_mu, update_beta, do_reparm;
     int do_reject, rejstart, rejint, maxrej;
     double lratemax, lnatrate, lratefact, rholrate, rhomin, rhomax, rejsig, ldetS;
+    int psi_is_phi;   // 1: the E-step's n x n slot already holds phi = sum g b^T (tensor-core form)
 };
 
 }  // namespace amica

@@ -31,12 +31,14 @@ cudaError_t launch_estep_plain(const EStepArgs& a, int NP, int nclusters, cudaSt
 int tc_supported(int n, int m, int M);
 int tc_max_clusters(int n, int m, int M);
 int tc_tile_samples();
+int tc_partial_groups();
+int tc_selftest(int mode, int N, int K, const float* hA, const float* hB, float* hD, int* derr);
 cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStream_t st);
 // preprocess.cu
 cudaError_t launch_preprocess(const float* raw, int64_t T, int n, int do_sphere, double* means,
                               double* cov, double* sphere, double* evwork, double* ldetS_dev,
-                              float* x, int ldx, cudaStream_t st);
-cudaError_t launch_convert_sphered(const double* xs, int64_t T, int n, float* x, int ldx,
+                              float* x, int ldx, int tf32, cudaStream_t st);
+cudaError_t launch_convert_sphered(const double* xs, int64_t T, int n, float* x, int ldx, int tf32,
                                    cudaStream_t st);
 // adjoint.cu
 cudaError_t launch_adjoint(const EStepArgs& a, int NP, double* grad_partial, int nclusters,
@@ -44,7 +46,7 @@ cudaError_t launch_adjoint(const EStepArgs& a, int NP, double* grad_partial, int
 cudaError_t launch_adjoint_finalize(const double* grad_partial, double* raw, int nclusters, int n,
                                     int m, int M, const double* A, const double* c,
                                     const double* beta, const double* rho, double* out,
-                                    cudaStream_t st);
+                                    int psi_is_phi, cudaStream_t st);
 
 cudaError_t launch_prep(const MStepBuffers& b, const MStepCfgHost& h, cudaStream_t st);
 cudaError_t launch_reduce_finalize(const MStepBuffers& b, const MStepCfgHost& h, int nclusters,
@@ -65,7 +67,7 @@ struct amica_ctx {
     int n = 0, M = 0, m = 0, NP = 0, S = 0;
     int64_t T = 0;
     bool use_tc = false;
-    int nclusters = 0, ntiles = 0;
+    int nclusters = 0, ntiles = 0, nslots = 0;   // nslots: partial-sum slots per model
     bool have_data = false, have_x = false, have_init = false, have_estep = false;
 
     float* d_rawx = nullptr;     // T x n raw input (float)
@@ -170,7 +172,7 @@ int enqueue_estep(amica_ctx* c) {
     EStepArgs a = estep_args(c);
     if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st));
     else CK(launch_estep_plain(a, c->NP, c->nclusters, c->st));
-    CK(launch_reduce_finalize(c->b, c->hc, c->nclusters, c->st));
+    CK(launch_reduce_finalize(c->b, c->hc, c->nslots, c->st));
     return AMICA_OK;
 }
 
@@ -325,6 +327,7 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     h.lratemax = cfg->lratemax; h.lnatrate = cfg->lnatrate; h.lratefact = cfg->lratefact;
     h.rholrate = cfg->rholrate; h.rhomin = cfg->rhomin; h.rhomax = cfg->rhomax;
     h.rejsig = cfg->rejsig; h.ldetS = 0.0;
+    h.psi_is_phi = c->use_tc ? 1 : 0;
 
     MStepBuffers& b = c->b;
     const size_t nn = (size_t)n * n, mn = (size_t)m * n;
@@ -334,7 +337,8 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     AL(b.beta, M * mn); AL(b.rho, M * mn); AL(b.gm, M); AL(b.W, M * nn); AL(b.ldet, M);
     AL(b.ltc64, M); AL(b.aug, M * nn * 2);
     PartLayout PL{(int)n, (int)m};
-    AL(b.partial, (size_t)c->nclusters * M * PL.stride());
+    c->nslots = c->nclusters * (c->use_tc ? tc_partial_groups() : 1);
+    AL(b.partial, (size_t)c->nslots * M * PL.stride());
     AL(b.raw, M * (size_t)PL.stride());
     AL(b.stats, (size_t)amica_stats_len(n, M, m));
     AL(b.work, M * 4 * n); AL(b.B, M * nn);
@@ -413,7 +417,8 @@ int amica_preprocess(amica_ctx* c) {
     if (!c->have_data) return AMICA_ERR_STATE;
     CK(cudaSetDevice(c->dev));
     CK(launch_preprocess(c->d_rawx, c->T, c->n, (int)c->cfg.do_sphere, c->d_means, c->d_cov,
-                         c->d_sphere, c->d_evwork, c->d_ldetS, c->d_x, c->NP, c->st));
+                         c->d_sphere, c->d_evwork, c->d_ldetS, c->d_x, c->NP, c->use_tc ? 1 : 0,
+                         c->st));
     double ld = 0.0;
     CK(cudaMemcpyAsync(&ld, c->d_ldetS, sizeof(double), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -432,7 +437,7 @@ int amica_set_sphered(amica_ctx* c, const double* xs, const double* means, const
     const size_t bytes = sizeof(double) * (size_t)c->T * c->n;
     CK(cudaMalloc(&tmp, bytes));
     CK(cudaMemcpyAsync(tmp, xs, bytes, cudaMemcpyHostToDevice, c->st));
-    CK(launch_convert_sphered(tmp, c->T, c->n, c->d_x, c->NP, c->st));
+    CK(launch_convert_sphered(tmp, c->T, c->n, c->d_x, c->NP, c->use_tc ? 1 : 0, c->st));
     if (means) CK(cudaMemcpyAsync(c->d_means, means, sizeof(double) * c->n, cudaMemcpyHostToDevice, c->st));
     if (sphere) CK(cudaMemcpyAsync(c->d_sphere, sphere, sizeof(double) * c->n * c->n, cudaMemcpyHostToDevice, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -682,8 +687,8 @@ int amica_loglik_adjoint(amica_ctx* c, double* ll, double* dW, double* dmu, doub
     CK(launch_prep(c->b, c->hc, c->st));
     EStepArgs a = estep_args(c);
     CK(launch_adjoint(a, c->NP, c->b.partial, c->nclusters, c->st, c->use_tc));
-    CK(launch_adjoint_finalize(c->b.partial, c->b.raw, c->nclusters, n, m, M, c->b.A, c->b.c,
-                               c->b.beta, c->b.rho, c->d_grad, c->st));
+    CK(launch_adjoint_finalize(c->b.partial, c->b.raw, c->nslots, n, m, M, c->b.A, c->b.c,
+                               c->b.beta, c->b.rho, c->d_grad, c->hc.psi_is_phi, c->st));
     TRY(check_device_error(c));
     std::vector<double> g(glen);
     CK(cudaMemcpy(g.data(), c->d_grad, sizeof(double) * glen, cudaMemcpyDeviceToHost));
@@ -794,6 +799,14 @@ int amica_write_outputs(amica_ctx* c, const amica_paths* p) {
 int amica_last_cuda_error(void) { return g_last_cuda_error; }
 
 int64_t amica_launches_per_iteration(amica_ctx* c) { return c ? launches_per_iteration(c) : 0; }
+
+int amica_selftest_umma(int mode, int N, int K, const float* A, const float* B, float* D,
+                        int* device_err) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return AMICA_ERR_NODEVICE;
+    if (!A || !B || !D || !device_err) return AMICA_ERR_INVALIDPARAM;
+    return tc_selftest(mode, N, K, A, B, D, device_err);
+}
 
 int amica_set_iter_state(amica_ctx* c, int64_t iter, double lrate, double ll_prev) {
     if (!c || iter < 0 || !(lrate > 0.0)) return AMICA_ERR_INVALIDPARAM;

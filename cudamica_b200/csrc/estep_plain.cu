@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
                     if (a.update_rho) fRn[j] = fmaf(u * p[j], pr[j] * L2[j] * kLn2, fRn[j]);
                 }
                 const float bb = bx - wci;
-                fCn = fmaf(v, xs[t * Sh::XLD + ch], fCn);
+                fCn = fmaf(v, bb, fCn);          // sum v b; cnew = A sum(v b) / vsum + c
                 fS2 = fmaf(v * bb, bb, fS2);
                 fGs += g;
                 gs[t * NP + ch] = ch_ok ? g : 0.f;

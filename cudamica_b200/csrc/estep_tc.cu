@@ -1,13 +1,929 @@
-// tcgen05 (TF32 tensor-core) form of the fused AMICA E-step: placeholder
-// until the tensor-core kernel lands; reports every shape as unsupported so
-// contexts fall back to the plain FP32 kernel.
+// Mixed-precision fused AMICA E-step on the 5th-generation tensor cores
+// (tcgen05, TF32 operands, FP32 accumulation in tensor memory).
+//
+// Cluster of M CTAs, CTA rank h = model h; persistent over 64-sample tiles.
+//   warp 16 (control): TMA loads of the x tile (128B-swizzled, two stages),
+//     and the two contractions issued by one thread:
+//       MMA1  b_h = W_hi x^T + W_lo x^T   M=128 (channels) N=48 (samples) K=n
+//             W_hi = tf32(W_h) K-major in smem, W_lo = tf32(W_h - W_hi) in TMEM,
+//             B = x tile (K-major, TMA), D -> TMEM (2 buffers)
+//       MMA2  phi_h += G B^T            M=128 N=n K=48
+//             A = G, B = the b tile, both K-major tiles written by the density
+//             warps, D -> TMEM for the CTA's life
+//   warps 0-15 (4 warpgroups x 4 warps): thread = (channel = TMEM lane,
+//     warpgroup = 16-sample slice).  Each reads its b values with tcgen05.ld,
+//     evaluates the generalized-Gaussian mixture densities and the log-sum-exp
+//     over mixtures (FP32, MUFU ex2/lg2), reduces over channels with warp
+//     shuffles, exchanges the per-sample Lt_h(t) with the other models' CTAs
+//     through distributed shared memory + remote mbarrier arrivals, forms
+//     P(t) and v_h(t), accumulates the sufficient statistics and writes
+//     g = sum_j sqrt(beta) u f' and b = W (x - c) into the MMA2 operand tiles.
+// (An MN-major TF32 operand needs the 32-byte-atom 128B swizzle, which the
+// x tile cannot have while it is also MMA1's K-major operand; so the second
+// contraction is phi = g b^T from two thread-written K-major tiles.)
+// The work of src/kernels.cu:227-827 and both cuBLAS Dgemm of the reference's
+// block loop (src/amica.cu:1054-1069, :1535-1550) happens in this one kernel.
+//
+// Every mbarrier wait is bounded (~1 s); on expiry the kernel records
+// kErrWaitTimeout, stops waiting, frees its tensor memory and exits.
+#include <cooperative_groups.h>
+#include <cuda.h>
+#include <cstdint>
+
 #include "common.cuh"
+
+namespace cg = cooperative_groups;
+using namespace amica;
+
+namespace {
+
+constexpr int kS = 48;                  // samples per tile (MMA1 N)
+constexpr int kWG = 3;                  // density warpgroups (13 warps: <= 128 registers)
+constexpr int kDensWarps = 4 * kWG;     // 12
+constexpr int kThreads = (kDensWarps + 1) * 32;
+constexpr int kSub = kS / kWG;          // 16 samples per thread per tile
+constexpr int kBcol = 64;               // TMEM column stride of the two b buffers
+constexpr int kPsiCol = 128;            // TMEM column of phi (N = NP columns)
+constexpr int kWloCol = 256;            // TMEM columns of W_lo, the A operand of the low MMA1 half
+constexpr int kFlush = 8;               // tiles between FP32 -> FP64 flushes
+constexpr long long kWaitCycles = 2000000000LL;   // ~1 s at 2 GHz
+
+// ---------------------------------------------------------------- PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok) : "r"(addr), "r"(parity) : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_try_cluster(uint32_t addr, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok) : "r"(addr), "r"(parity) : "memory");
+    return ok != 0;
+}
+// bounded wait: false on timeout or when another thread already aborted
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                          int* err, bool cluster_scope = false,
+                                          bool honor_abort = true) {
+    const uint32_t addr = smem_u32(bar);
+    long long t0 = clock64();
+    while (true) {
+        if (cluster_scope ? mbar_try_cluster(addr, parity) : mbar_try(addr, parity)) return true;
+        if (honor_abort && *abort_flag) return false;
+        if (clock64() - t0 > kWaitCycles) {
+            *abort_flag = 1;
+            atomicOr(err, kErrWaitTimeout);
+            return false;
+        }
+    }
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ uint32_t mapa(uint32_t addr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void st_cluster_f32(uint32_t addr, float v) {
+    asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(addr), "f"(v) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t addr) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(addr) : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(dst), "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void tc_mma_tf32(uint32_t dtmem, uint64_t adesc, uint64_t bdesc,
+                                            uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(dtmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate) : "memory");
+}
+__device__ __forceinline__ void tc_mma_tf32_ta(uint32_t dtmem, uint32_t atmem, uint64_t bdesc,
+                                               uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}"
+        ::"r"(dtmem), "r"(atmem), "l"(bdesc), "r"(idesc), "r"(accumulate) : "memory");
+}
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+        "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
+        ::"r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+          "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+          "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+          "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+          "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+          "r"(__float_as_uint(v[15]))
+        : "memory");
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 16; q++) v[q] = __uint_as_float(r[q]);
+}
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, float* v) {
+    uint32_t r0, r1, r2, r3;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    v[0] = __uint_as_float(r0); v[1] = __uint_as_float(r1);
+    v[2] = __uint_as_float(r2); v[3] = __uint_as_float(r3);
+}
+__device__ __forceinline__ float tf32_rna(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// Shared-memory matrix descriptor, SWIZZLE_128B, sm100 version bits.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+// Instruction descriptor, kind::tf32, D=F32, A=B=TF32.
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N, int a_mn_major, int b_mn_major) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)a_mn_major << 15) |
+           ((uint32_t)b_mn_major << 16) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// Offset (bytes) of element (row, col) in a K-major SW128 tile of 32-bit
+// elements whose 128-byte rows hold 32 consecutive columns; column blocks of
+// `rows` x 128 B follow each other.
+__device__ __forceinline__ uint32_t sw128_off(int row, int col, int rows) {
+    const int blk = col >> 5, c = col & 31;
+    return (uint32_t)(blk * rows * 128 + row * 128 + ((((c >> 2) ^ (row & 7)) & 7) << 4) + ((c & 3) << 2));
+}
+
+template <int NP>
+struct TcShape {
+    static constexpr int KB = NP / 32;                       // 128-B column blocks of x / W
+    static constexpr uint32_t W_BYTES = 128u * NP * 4u;      // 128 rows x NP
+    static constexpr uint32_t X_BYTES = (uint32_t)kS * NP * 4u;
+    static constexpr uint32_t G_BYTES = 128u * 128u * 2u;    // 128 rows x 2 blocks of 32 samples
+    static constexpr uint32_t OFF_W = 0;
+    static constexpr uint32_t OFF_X0 = OFF_W + W_BYTES;
+    static constexpr uint32_t OFF_X1 = OFF_X0 + X_BYTES;
+    static constexpr uint32_t OFF_G = OFF_X1 + X_BYTES;
+    static constexpr uint32_t OFF_BT = OFF_G + G_BYTES;                  // b tile, same layout as G
+    static constexpr uint32_t OFF_RED = OFF_BT + G_BYTES;                // [2][WG][4 warps][16] f32
+    static constexpr uint32_t OFF_SLOT = OFF_RED + 2 * kWG * 4 * 16 * 4;  // [2][8 models][64] f32
+    static constexpr uint32_t OFF_BAR = OFF_SLOT + 2 * kMaxModels * kS * 4;
+    static constexpr uint32_t NBAR = 24;
+    static constexpr uint32_t OFF_MISC = OFF_BAR + NBAR * 8;
+    static constexpr uint32_t BYTES = OFF_MISC + 64;
+    static constexpr uint32_t TMEM_COLS = 512;   // b: [0,48) [64,112); phi: [128,128+NP); W_lo: [256,256+NP)
+};
+
+enum { BAR_FULL0 = 0, BAR_FULL1, BAR_EMPTY0, BAR_EMPTY1, BAR_BFULL0, BAR_BFULL1, BAR_BEMPTY0,
+       BAR_BEMPTY1, BAR_GFULL, BAR_GEMPTY, BAR_LT0, BAR_LT1, BAR_PSI, BAR_DRAIN,
+       BAR_RED0 /* 2 parities x kWG warpgroups: BAR_RED0 + par * kWG + wg */ };
+
+struct TcArgs {
+    EStepArgs e;
+    int ngroups;   // partial slots per cluster (one per warpgroup)
+};
+
+template <int NP, int MM>
+__global__ void __launch_bounds__(kThreads, 1)
+    estep_tc_kernel(const __grid_constant__ CUtensorMap xmap, TcArgs ta) {
+    using Sh = TcShape<NP>;
+    const EStepArgs& a = ta.e;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    // 1024-byte alignment for the swizzled operand tiles
+    uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    float* Wsm = (float*)(sm + Sh::OFF_W);
+    float* Gsm = (float*)(sm + Sh::OFF_G);
+    float* red = (float*)(sm + Sh::OFF_RED);
+    float* slot = (float*)(sm + Sh::OFF_SLOT);
+    uint64_t* bar = (uint64_t*)(sm + Sh::OFF_BAR);
+    uint32_t* tmem_holder = (uint32_t*)(sm + Sh::OFF_MISC);
+    volatile int* abort_flag = (volatile int*)(sm + Sh::OFF_MISC + 8);
+
+    cg::cluster_group cluster = cg::this_cluster();
+    const int h = (int)cluster.block_rank();
+    const int M = a.M, n = a.n;
+    const int cid = blockIdx.x / M;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ntile_local = (a.ntiles > cid) ? (a.ntiles - cid + a.nclusters - 1) / a.nclusters : 0;
+
+    // ---- setup: barriers, W_h into the swizzled A tile, tensor memory
+    if (tid == 0) {
+        mbar_init(&bar[BAR_FULL0], 1);
+        mbar_init(&bar[BAR_FULL1], 1);
+        mbar_init(&bar[BAR_EMPTY0], 1);
+        mbar_init(&bar[BAR_EMPTY1], 1);
+        mbar_init(&bar[BAR_BFULL0], 1);
+        mbar_init(&bar[BAR_BFULL1], 1);
+        mbar_init(&bar[BAR_BEMPTY0], kDensWarps);
+        mbar_init(&bar[BAR_BEMPTY1], kDensWarps);
+        mbar_init(&bar[BAR_GFULL], kDensWarps);
+        mbar_init(&bar[BAR_GEMPTY], 1);
+        mbar_init(&bar[BAR_LT0], (uint32_t)(16 * kWG * M));
+        mbar_init(&bar[BAR_LT1], (uint32_t)(16 * kWG * M));
+        mbar_init(&bar[BAR_PSI], 1);
+        mbar_init(&bar[BAR_DRAIN], 1);
+        for (int r = 0; r < 2 * kWG; r++) mbar_init(&bar[BAR_RED0 + r], 4);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    {
+        const float* Wh = a.Wf + (size_t)h * NP * NP;   // W[i][k], rows i >= NP are zero
+        for (int e4 = tid; e4 < 128 * (NP / 4); e4 += kThreads) {
+            const int i = e4 / (NP / 4), k = (e4 % (NP / 4)) * 4;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (i < NP) v = *reinterpret_cast<const float4*>(Wh + (size_t)i * NP + k);
+            v.x = tf32_rna(v.x); v.y = tf32_rna(v.y); v.z = tf32_rna(v.z); v.w = tf32_rna(v.w);
+            *reinterpret_cast<float4*>((uint8_t*)Wsm + sw128_off(i, k, 128)) = v;
+        }
+    }
+    if (warp == kDensWarps) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(tmem_holder)), "r"(Sh::TMEM_COLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_proxy_async();                 // W tile written by generic stores -> async proxy
+    tc_fence_before();
+    cluster.sync();                      // barriers of every CTA initialised before remote use
+    tc_fence_after();
+    const uint32_t tmem = *tmem_holder;
+    const uint32_t tmem_b0 = tmem, tmem_psi = tmem + kPsiCol;
+    // W_lo = W - tf32(W) into tensor memory (row i -> lane i): the A operand of the
+    // second half of MMA1, so that b = W_hi x + W_lo x keeps W to ~2^-22
+    if (warp < 4) {
+        const int i = warp * 32 + lane;
+        const float* Wrow = a.Wf + ((size_t)h * NP + (i < NP ? i : 0)) * NP;
+#pragma unroll 1
+        for (int k0 = 0; k0 < NP; k0 += 16) {
+            float lo[16];
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+                const float w = (i < NP) ? Wrow[k0 + q] : 0.f;
+                lo[q] = tf32_rna(w - tf32_rna(w));
+            }
+            tmem_st16(tmem + kWloCol + ((uint32_t)(warp * 32) << 16) + (uint32_t)k0, lo);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+
+    if (warp == kDensWarps) {
+        // =========================== control warp: TMA + MMA =====================
+        if (lane == 0 && ntile_local > 0) {
+            const uint32_t x_off[2] = {Sh::OFF_X0, Sh::OFF_X1};
+            const uint32_t sbase = smem_u32(sm);
+            auto issue_tma = [&](int k) {
+                const int s = k & 1;
+                const int64_t tile = (int64_t)cid + (int64_t)k * a.nclusters;
+                mbar_expect_tx(&bar[BAR_FULL0 + s], Sh::X_BYTES);
+#pragma unroll
+                for (int cb = 0; cb < Sh::KB; cb++)
+                    tma_load_2d(sbase + x_off[s] + cb * kS * 128, &xmap, cb * 32, (int)(tile * kS),
+                                &bar[BAR_FULL0 + s]);
+            };
+            constexpr uint32_t ID1 = idesc_tf32(128, kS, 0, 0);
+            constexpr uint32_t ID2 = idesc_tf32(128, NP, 0, 0);
+            int issued = 0, consumed = 0;
+            issue_tma(0);
+            issued = 1;
+            if (ntile_local > 1) { issue_tma(1); issued = 2; }
+            bool ok = true;
+            for (int k = 0; k < ntile_local && ok; k++) {
+                const int s = k & 1;
+                const uint32_t u = (uint32_t)(k >> 1);
+                // MMA1 for tile k: needs x stage s and a free b buffer
+                ok = mbar_wait(&bar[BAR_FULL0 + s], u & 1, abort_flag, a.err);
+                if (ok) consumed = k + 1;
+                if (ok && k >= 2) ok = mbar_wait(&bar[BAR_BEMPTY0 + s], (u - 1) & 1, abort_flag, a.err);
+                if (!ok) break;
+                tc_fence_after();
+                const uint32_t xb = sbase + x_off[s];
+#pragma unroll
+                for (int kk = 0; kk < NP / 8; kk++) {
+                    const uint32_t koff = (uint32_t)((kk >> 2) * 0) + (uint32_t)((kk & 3) * 32);
+                    const uint64_t ad = sdesc(sbase + Sh::OFF_W + (kk >> 2) * 128 * 128 + koff, 16, 1024);
+                    const uint64_t bd = sdesc(xb + (kk >> 2) * kS * 128 + koff, 16, 1024);
+                    tc_mma_tf32(tmem_b0 + s * kBcol, ad, bd, ID1, kk > 0 ? 1u : 0u);
+                }
+#pragma unroll
+                for (int kk = 0; kk < NP / 8; kk++) {
+                    const uint64_t bd = sdesc(xb + (kk >> 2) * kS * 128 + (uint32_t)((kk & 3) * 32), 16, 1024);
+                    tc_mma_tf32_ta(tmem_b0 + s * kBcol, tmem + kWloCol + (uint32_t)(kk * 8), bd, ID1, 1u);
+                }
+                tc_commit(&bar[BAR_BFULL0 + s]);
+                // MMA2 for tile k-1: needs its G tile
+                if (k >= 1) {
+                    const int kp = k - 1, sp = kp & 1;
+                    ok = mbar_wait(&bar[BAR_GFULL], (uint32_t)(kp & 1), abort_flag, a.err);
+                    if (!ok) break;
+                    tc_fence_after();
+#pragma unroll
+                    for (int kk = 0; kk < kS / 8; kk++) {
+                        const uint64_t ad = sdesc(sbase + Sh::OFF_G + (kk >> 2) * 128 * 128 + (kk & 3) * 32, 16, 1024);
+                        const uint64_t bd = sdesc(sbase + Sh::OFF_BT + (kk >> 2) * 128 * 128 + (kk & 3) * 32, 16, 1024);
+                        tc_mma_tf32(tmem_psi, ad, bd, ID2, (kp > 0 || kk > 0) ? 1u : 0u);
+                    }
+                    tc_commit(&bar[BAR_EMPTY0 + sp]);
+                    tc_commit(&bar[BAR_GEMPTY]);
+                    // stage sp is refilled with tile k+1 once MMA2(k-1) has read it
+                    if (k + 1 < ntile_local) {
+                        ok = mbar_wait(&bar[BAR_EMPTY0 + sp], (uint32_t)((kp >> 1) & 1), abort_flag, a.err);
+                        if (!ok) break;
+                        issue_tma(k + 1);
+                        issued = k + 2;
+                    }
+                }
+            }
+            // MMA2 for the last tile
+            if (ok) {
+                const int kp = ntile_local - 1, sp = kp & 1;
+                ok = mbar_wait(&bar[BAR_GFULL], (uint32_t)(kp & 1), abort_flag, a.err);
+                if (ok) {
+                    tc_fence_after();
+#pragma unroll
+                    for (int kk = 0; kk < kS / 8; kk++) {
+                        const uint64_t ad = sdesc(sbase + Sh::OFF_G + (kk >> 2) * 128 * 128 + (kk & 3) * 32, 16, 1024);
+                        const uint64_t bd = sdesc(sbase + Sh::OFF_BT + (kk >> 2) * 128 * 128 + (kk & 3) * 32, 16, 1024);
+                        tc_mma_tf32(tmem_psi, ad, bd, ID2, (kp > 0 || kk > 0) ? 1u : 0u);
+                    }
+                    tc_commit(&bar[BAR_PSI]);
+                }
+            }
+            // drain: every TMA load this thread issued has landed and every MMA it
+            // issued has completed before the CTA frees tensor memory (bounded)
+            for (int t = consumed; t < issued; t++)
+                mbar_wait(&bar[BAR_FULL0 + (t & 1)], (uint32_t)((t >> 1) & 1), abort_flag, a.err, false,
+                          false);
+            tc_commit(&bar[BAR_DRAIN]);
+            mbar_wait(&bar[BAR_DRAIN], 0u, abort_flag, a.err, false, false);
+        }
+        __syncwarp();
+    } else {
+        // =========================== density warps =================================
+        const int wg = warp >> 2, q4 = warp & 3;
+        const int ch = q4 * 32 + lane;             // channel = TMEM lane
+        const bool ch_ok = ch < n;
+        const uint32_t lane_addr = (uint32_t)(q4 * 32) << 16;
+        float ps[MM], po[MM], pc[MM], pr[MM];
+#pragma unroll
+        for (int j = 0; j < MM; j++) {
+            const MixParam q = a.mp[((size_t)h * MM + j) * NP + (ch < NP ? ch : 0)];
+            ps[j] = ch < NP ? q.s : 0.f; po[j] = ch < NP ? q.off : 0.f;
+            pc[j] = ch < NP ? q.cl2 : 0.f; pr[j] = ch < NP ? q.rho : 1.f;
+        }
+        const float wci = ch < NP ? a.wc[(size_t)h * NP + ch] : 0.f;
+        const float ltc_h = (float)(a.ltc64[h] - a.ltc64[0]);
+        float ltc_all[kMaxModels];
+#pragma unroll
+        for (int q = 0; q < kMaxModels; q++) ltc_all[q] = (q < M) ? (float)(a.ltc64[q] - a.ltc64[0]) : 0.f;
+        (void)ltc_all;
+
+        float fUs[MM], fKn[MM], fLn[MM], fMn[MM], fMd[MM], fBd[MM], fRn[MM];
+        float fCn = 0.f, fS2 = 0.f, fGs = 0.f;
+#pragma unroll
+        for (int j = 0; j < MM; j++) fUs[j] = fKn[j] = fLn[j] = fMn[j] = fMd[j] = fBd[j] = fRn[j] = 0.f;
+        double dLL = 0.0, dVs = 0.0;
+        // this thread's partial slot (one per warpgroup)
+        PartLayout L{n, MM};
+        double* out = a.partial + ((size_t)(cid * ta.ngroups + wg) * M + h) * L.stride();
+        double* out0 = a.partial + ((size_t)(cid * ta.ngroups) * M + h) * L.stride();  // Psi lives here
+        auto flush = [&]() {
+            if (ch_ok) {
+#pragma unroll
+                for (int j = 0; j < MM; j++) {
+                    out[L.mix(kUs) + j * n + ch] += fUs[j];
+                    out[L.mix(kKn) + j * n + ch] += fKn[j];
+                    out[L.mix(kLn) + j * n + ch] += fLn[j];
+                    out[L.mix(kMn) + j * n + ch] += fMn[j];
+                    out[L.mix(kMd) + j * n + ch] += fMd[j];
+                    out[L.mix(kBd) + j * n + ch] += fBd[j];
+                    out[L.mix(kRn) + j * n + ch] += fRn[j];
+                }
+                out[L.cn() + ch] += fCn;
+                out[L.s2() + ch] += fS2;
+                out[L.gs() + ch] += fGs;
+            }
+#pragma unroll
+            for (int j = 0; j < MM; j++) fUs[j] = fKn[j] = fLn[j] = fMn[j] = fMd[j] = fBd[j] = fRn[j] = 0.f;
+            fCn = fS2 = fGs = 0.f;
+        };
+        // zero this thread's fields of the slot
+        if (ch_ok) {
+            for (int k = 0; k < 7 * MM; k++) out[L.mix(0) + k * n + ch] = 0.0;
+            out[L.cn() + ch] = 0.0;
+            out[L.s2() + ch] = 0.0;
+            out[L.gs() + ch] = 0.0;
+        }
+        bool ok = true;
+        for (int k = 0; k < ntile_local && ok; k++) {
+            const int s = k & 1;
+            const uint32_t u = (uint32_t)(k >> 1);
+            const int64_t t0 = ((int64_t)cid + (int64_t)k * a.nclusters) * kS + wg * kSub;
+            ok = mbar_wait(&bar[BAR_BFULL0 + s], u & 1, abort_flag, a.err);
+            if (!ok) break;
+            tc_fence_after();
+            const uint32_t bcol = tmem_b0 + lane_addr + (uint32_t)(s * kBcol + wg * kSub);
+
+            // ---- phase 1: per-sample log-sum-exp over mixtures (log2 units), 4 samples at a
+            // time; the channel sum per sample is a 4-value transposed butterfly over the
+            // warp's 32 lanes, after which lane 8q holds the warp's sum for sample 4g+q
+#pragma unroll 1
+            for (int g4 = 0; g4 < kSub / 4; g4++) {
+                float bx[4], v[4];
+                tmem_ld4(bcol + (uint32_t)(g4 * 4), bx);
+#pragma unroll
+                for (int r = 0; r < 4; r++) {
+                    float q[MM], qmax = -INFINITY;
+#pragma unroll
+                    for (int j = 0; j < MM; j++) {
+                        const float y = fmaf(ps[j], bx[r], -po[j]);
+                        const float ay = fmaxf(fabsf(y), kTinyAbs);
+                        const float p = ptx_ex2(pr[j] * ptx_lg2(ay));
+                        q[j] = fmaf(-p, kLog2e, pc[j]);
+                        qmax = fmaxf(qmax, q[j]);
+                    }
+                    float se = 0.f;
+#pragma unroll
+                    for (int j = 0; j < MM; j++) se += ptx_ex2(q[j] - qmax);
+                    v[r] = ch_ok ? qmax + ptx_lg2(se) : 0.f;
+                }
+                {
+                    const bool up16 = (lane & 16) != 0;
+                    const float s0 = up16 ? v[0] : v[2], s1 = up16 ? v[1] : v[3];
+                    const float k0 = up16 ? v[2] : v[0], k1 = up16 ? v[3] : v[1];
+                    v[0] = k0 + __shfl_xor_sync(0xffffffffu, s0, 16);
+                    v[1] = k1 + __shfl_xor_sync(0xffffffffu, s1, 16);
+                    const bool up8 = (lane & 8) != 0;
+                    const float s2 = up8 ? v[0] : v[1], k2 = up8 ? v[1] : v[0];
+                    float w = k2 + __shfl_xor_sync(0xffffffffu, s2, 8);
+                    w += __shfl_xor_sync(0xffffffffu, w, 4);
+                    w += __shfl_xor_sync(0xffffffffu, w, 2);
+                    w += __shfl_xor_sync(0xffffffffu, w, 1);
+                    // lane bits (4,3) select the sample: 2*bit4 + bit3
+                    if ((lane & 7) == 0)
+                        red[(((k & 1) * kWG + wg) * 4 + q4) * 16 + g4 * 4 + ((lane >> 4) & 1) * 2 +
+                            ((lane >> 3) & 1)] = w;
+                }
+            }
+            // the four warps of this warpgroup combine; lanes 0-15 of warp q4 == 0 publish
+            const int par = k & 1;
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bar[BAR_RED0 + par * kWG + wg]);
+            if (q4 == 0) {
+                ok = mbar_wait(&bar[BAR_RED0 + par * kWG + wg], u & 1, abort_flag, a.err);
+                if (!ok) break;
+            }
+            if (q4 == 0 && lane < 16) {
+                const float* rr = red + ((par * kWG + wg) * 4) * 16;
+                const float s4 = rr[0 * 16 + lane] + rr[1 * 16 + lane] + rr[2 * 16 + lane] + rr[3 * 16 + lane];
+                const float Lh = ltc_h + kLn2 * s4;
+                const uint32_t sl = smem_u32(slot + (par * kMaxModels + h) * kS + wg * kSub + lane);
+                const uint32_t lb = smem_u32(&bar[BAR_LT0 + par]);
+                for (int q = 0; q < M; q++) {
+                    st_cluster_f32(mapa(sl, (uint32_t)q), Lh);
+                    mbar_arrive_remote(mapa(lb, (uint32_t)q));
+                }
+            }
+            ok = mbar_wait(&bar[BAR_LT0 + par], u & 1, abort_flag, a.err, true);
+            if (!ok) break;
+            // ---- P(t), v_h(t): lanes 0-15 of every warp, one sample each
+            float vme = 0.f;
+            {
+                const int t = lane & 15;
+                float Lq[kMaxModels];
+                float lmax = -INFINITY;
+#pragma unroll
+                for (int q = 0; q < kMaxModels; q++) {
+                    if (q < M) {
+                        Lq[q] = slot[(par * kMaxModels + q) * kS + wg * kSub + t];
+                        lmax = fmaxf(lmax, Lq[q]);
+                    }
+                }
+                float se = 0.f;
+#pragma unroll
+                for (int q = 0; q < kMaxModels; q++)
+                    if (q < M) se += ptx_ex2((Lq[q] - lmax) * kLog2e);
+                const float P = lmax + kLn2 * ptx_lg2(se);
+                float Lmine = 0.f;
+#pragma unroll
+                for (int q = 0; q < kMaxModels; q++)
+                    if (q == h) Lmine = Lq[q];
+                const float vh = ptx_ex2((Lmine - P) * kLog2e);
+                const int64_t tg = t0 + t;
+                const bool valid = tg < a.T && (a.keep == nullptr || a.keep[tg]);
+                vme = valid ? vh : 0.f;
+                if (q4 == 0 && lane < 16) {
+                    if (valid) {
+                        dVs += (double)vh;
+                        if (h == 0) dLL += (double)P;
+                    }
+                    if (tg < a.T) {
+                        if (a.Lt_out) a.Lt_out[(size_t)h * a.T + tg] = Lmine;
+                        if (a.P_out && h == 0) a.P_out[tg] = P;
+                    }
+                }
+            }
+            // ---- phase 2 (G tile is free once MMA2 of the previous tile has run)
+            if (k >= 1) {
+                ok = mbar_wait(&bar[BAR_GEMPTY], (uint32_t)((k - 1) & 1), abort_flag, a.err);
+                if (!ok) break;
+            }
+#pragma unroll 1
+            for (int g4 = 0; g4 < kSub / 4; g4++) {
+                float bx[4], gq[4], bq[4];
+                tmem_ld4(bcol + (uint32_t)(g4 * 4), bx);
+#pragma unroll
+                for (int r = 0; r < 4; r++) {
+                    const float v = __shfl_sync(0xffffffffu, vme, g4 * 4 + r);
+                    float y[MM], L2[MM], p[MM], q[MM], qmax = -INFINITY;
+#pragma unroll
+                    for (int j = 0; j < MM; j++) {
+                        y[j] = fmaf(ps[j], bx[r], -po[j]);
+                        const float ay = fmaxf(fabsf(y[j]), kTinyAbs);
+                        L2[j] = ptx_lg2(ay);
+                        p[j] = ptx_ex2(pr[j] * L2[j]);
+                        q[j] = fmaf(-p[j], kLog2e, pc[j]);
+                        qmax = fmaxf(qmax, q[j]);
+                    }
+                    float e[MM], se = 0.f;
+#pragma unroll
+                    for (int j = 0; j < MM; j++) { e[j] = ptx_ex2(q[j] - qmax); se += e[j]; }
+                    const float vr = v * ptx_rcp(se);
+                    float g = 0.f;
+#pragma unroll
+                    for (int j = 0; j < MM; j++) {
+                        const float uu = e[j] * vr;
+                        const float ay = fmaxf(fabsf(y[j]), kTinyAbs);
+                        const float ri = ptx_rcp(ay);
+                        const float pm1 = p[j] * ri;
+                        const float fp = copysignf(pr[j] * pm1, y[j]);
+                        const float ufp = uu * fp;
+                        g = fmaf(ps[j], ufp, g);
+                        fUs[j] += uu;
+                        fKn[j] = fmaf(ufp, fp, fKn[j]);
+                        const float lv = fmaf(fp, y[j], -1.f);
+                        fLn[j] = fmaf(uu * lv, lv, fLn[j]);
+                        fMn[j] += ufp;
+                        if (pr[j] <= 2.f || a.grad_mode) {
+                            fMd[j] = fmaf(ufp, copysignf(ri, y[j]), fMd[j]);
+                            fBd[j] = fmaf(ufp, y[j], fBd[j]);
+                        } else {
+                            fMd[j] = fmaf(ufp, fp, fMd[j]);
+                            fBd[j] = fmaf(uu, p[j], fBd[j]);
+                        }
+                        if (a.update_rho) fRn[j] = fmaf(uu * p[j], pr[j] * L2[j] * kLn2, fRn[j]);
+                    }
+                    const float bb = bx[r] - wci;
+                    fCn = fmaf(v, bb, fCn);
+                    fS2 = fmaf(v * bb, bb, fS2);
+                    g = ch_ok ? g : 0.f;
+                    fGs += g;
+                    gq[r] = tf32_rna(g);
+                    bq[r] = ch_ok ? tf32_rna(bb) : 0.f;
+                }
+                const uint32_t goff = sw128_off(ch, wg * kSub + g4 * 4, 128);
+                *reinterpret_cast<float4*>((uint8_t*)Gsm + goff) = make_float4(gq[0], gq[1], gq[2], gq[3]);
+                *reinterpret_cast<float4*>(sm + Sh::OFF_BT + goff) = make_float4(bq[0], bq[1], bq[2], bq[3]);
+            }
+            // b buffer s fully consumed: release it to MMA1 of tile k+2
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bar[BAR_BEMPTY0 + s]);
+            fence_proxy_async();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bar[BAR_GFULL]);
+            if ((k + 1) % kFlush == 0) flush();
+        }
+        flush();
+        // vsum / LL of this warpgroup (warp q4 == 0 accumulated them)
+        if (q4 == 0) {
+            double a1 = dLL, a2 = dVs;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+                a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+            }
+            if (lane == 0) {
+                out[0] = a1;
+                out[1] = a2;
+            }
+        }
+        // ---- Psi_h out of tensor memory: warpgroup wg reads columns [wg*NP/4, (wg+1)*NP/4)
+        if (ok && ntile_local > 0) ok = mbar_wait(&bar[BAR_PSI], 0u, abort_flag, a.err);
+        if (ok && ntile_local > 0) {
+            tc_fence_after();
+            // 16-column chunks of Psi, dealt round-robin to the warpgroups
+#pragma unroll
+            for (int c0 = 0; c0 < NP; c0 += 16) {
+                if ((c0 / 16) % kWG != wg) continue;
+                float v[16];
+                tmem_ld16(tmem_psi + lane_addr + (uint32_t)c0, v);
+#pragma unroll
+                for (int q = 0; q < 16; q++) {
+                    const int kcol = c0 + q;
+                    if (ch_ok && kcol < n) out0[L.psi() + (size_t)kcol * n + ch] = (double)v[q];
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    cluster.sync();
+    if (warp == kDensWarps) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     ::"r"(tmem), "r"(Sh::TMEM_COLS) : "memory");
+    }
+}
+
+// ---------------------------------------------------------------- self-test
+// One CTA runs a single contraction D[128][N] = A[128][K] . B[N][K]^T with the
+// layouts, descriptors and TMEM access of the E-step kernel (B K-major in
+// shared memory, as the x tile in MMA1 and the b tile in MMA2):
+//   mode 0: A = tf32(A) K-major in shared memory (W_hi, G)
+//   mode 1: A = tf32(A) in tensor memory (the A-from-TMEM form of W_lo)
+//   mode 2: A = hi + lo split, hi in shared memory, lo in tensor memory (MMA1)
+// K is a multiple of 16 (<= 64); N a multiple of 16 (<= 128).
+__global__ void __launch_bounds__(128, 1) umma_selftest_kernel(const float* __restrict__ A,
+                                                               const float* __restrict__ B,
+                                                               float* __restrict__ D, int mode,
+                                                               int N, int K, int* err) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* As = sm;                      // K-major, 128 rows, ceil(K/32) blocks of 16 KB
+    uint8_t* Bs = sm + 2 * 16384;          // K-major, N rows
+    uint64_t* bar = (uint64_t*)(sm + 2 * 16384 + 2 * 16384);
+    uint32_t* holder = (uint32_t*)(bar + 2);
+    volatile int* abort_flag = (volatile int*)(bar + 3);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int e = tid; e < 128 * K; e += 128) {
+        const int r = e / K, c = e % K;
+        *(float*)(As + sw128_off(r, c, 128)) = tf32_rna(A[e]);
+    }
+    for (int e = tid; e < N * K; e += 128) {
+        const int r = e / K, c = e % K;
+        *(float*)(Bs + sw128_off(r, c, N)) = tf32_rna(B[e]);
+    }
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(holder)), "r"(128u) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *holder;                     // D: columns [0, N); A in TMEM: [N, N+K)
+    if (mode >= 1) {
+        const int r = warp * 32 + lane;
+        for (int k0 = 0; k0 < K; k0 += 16) {
+            float v[16];
+            for (int q = 0; q < 16; q++) {
+                const float w = A[(size_t)r * K + k0 + q];
+                v[q] = mode == 1 ? tf32_rna(w) : tf32_rna(w - tf32_rna(w));
+            }
+            tmem_st16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(N + k0), v);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (tid == 0) {
+        const uint32_t abase = smem_u32(As), bbase = smem_u32(Bs);
+        const uint32_t id = idesc_tf32(128, N, 0, 0);
+        for (int kk = 0; kk < K / 8; kk++) {
+            const uint64_t bd = sdesc(bbase + (kk >> 2) * N * 128 + (kk & 3) * 32, 16, 1024);
+            if (mode == 0 || mode == 2) {
+                const uint64_t ad = sdesc(abase + (kk >> 2) * 128 * 128 + (kk & 3) * 32, 16, 1024);
+                tc_mma_tf32(tmem, ad, bd, id, kk > 0 ? 1u : 0u);
+            }
+            if (mode >= 1)
+                tc_mma_tf32_ta(tmem, tmem + (uint32_t)(N + kk * 8), bd, id,
+                               (mode == 2 || kk > 0) ? 1u : 0u);
+        }
+        tc_commit(&bar[0]);
+    }
+    __syncwarp();
+    const bool ok = mbar_wait(&bar[0], 0u, abort_flag, err);
+    tc_fence_after();
+    if (ok) {
+        for (int c0 = 0; c0 < N; c0 += 16) {
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            for (int q = 0; q < 16; q++) D[(size_t)(warp * 32 + lane) * N + c0 + q] = v[q];
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128u)
+                     : "memory");
+    }
+}
+
+// ---------------------------------------------------------------- host side
+typedef CUresult (*PFN_encodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                    const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                    const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                    CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+PFN_encodeTiled get_encode() {
+    static PFN_encodeTiled fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_encodeTiled)p;
+    }
+    return fn;
+}
+
+template <int NP, int MM>
+cudaError_t launch_tc(const EStepArgs& a, int nclusters, cudaStream_t st) {
+    using Sh = TcShape<NP>;
+    PFN_encodeTiled enc = get_encode();
+    if (!enc) return cudaErrorNotSupported;
+    CUtensorMap map;
+    cuuint64_t dims[2] = {(cuuint64_t)a.ldx, (cuuint64_t)a.T};
+    cuuint64_t strides[1] = {(cuuint64_t)a.ldx * 4};
+    cuuint32_t box[2] = {32, (cuuint32_t)kS};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)a.x, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    const size_t smem = Sh::BYTES + 1024;
+    auto kern = estep_tc_kernel<NP, MM>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    TcArgs ta;
+    ta.e = a;
+    ta.ngroups = kWG;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nclusters * a.M);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = a.M;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, map, ta);
+}
+
+template <int NP, int MM>
+int tc_active_clusters(int M) {
+    using Sh = TcShape<NP>;
+    const size_t smem = Sh::BYTES + 1024;
+    auto kern = estep_tc_kernel<NP, MM>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return -1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(M * 64);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = M;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int num = 0;
+    if (cudaOccupancyMaxActiveClusters(&num, kern, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    return num;
+}
+
+}  // namespace
 
 namespace amica {
 
-int tc_supported(int, int, int) { return 0; }
-int tc_max_clusters(int, int, int) { return -1; }
-int tc_tile_samples() { return 128; }
-cudaError_t launch_estep_tc(const EStepArgs&, int, int, cudaStream_t) { return cudaErrorNotSupported; }
+int tc_selftest(int mode, int N, int K, const float* hA, const float* hB, float* hD, int* derr) {
+    if (mode < 0 || mode > 2 || N % 16 || N < 16 || N > 64 || K % 16 || K < 16 || K > 64)
+        return -3;
+    float *dA, *dB, *dD;
+    int* err;
+    if (cudaMalloc(&dA, sizeof(float) * 128 * K) != cudaSuccess) return -1;
+    cudaMalloc(&dB, sizeof(float) * N * K);
+    cudaMalloc(&dD, sizeof(float) * 128 * N);
+    cudaMalloc(&err, sizeof(int));
+    cudaMemset(err, 0, sizeof(int));
+    cudaMemcpy(dA, hA, sizeof(float) * 128 * K, cudaMemcpyHostToDevice);
+    cudaMemcpy(dB, hB, sizeof(float) * N * K, cudaMemcpyHostToDevice);
+    const int smem = 4 * 16384 + 1024 + 64;
+    cudaFuncSetAttribute(umma_selftest_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    umma_selftest_kernel<<<1, 128, smem>>>(dA, dB, dD, mode, N, K, err);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) {
+        cudaMemcpy(hD, dD, sizeof(float) * 128 * N, cudaMemcpyDeviceToHost);
+        cudaMemcpy(derr, err, sizeof(int), cudaMemcpyDeviceToHost);
+    }
+    cudaFree(dA); cudaFree(dB); cudaFree(dD); cudaFree(err);
+    return e == cudaSuccess ? 0 : -20;
+}
+
+int tc_tile_samples() { return kS; }
+int tc_partial_groups() { return kWG; }
+
+int tc_supported(int n, int m, int M) {
+    return n >= 2 && n <= 128 && m >= 1 && m <= 5 && M >= 1 && M <= kMaxModels;
+}
+
+static int tc_np(int n) { return n <= 32 ? 32 : (n <= 64 ? 64 : 128); }
+
+int tc_max_clusters(int n, int m, int M) {
+    if (!tc_supported(n, m, M)) return -1;
+    const int NP = tc_np(n);
+#define AMICA_TC_OCC(NPV, MMV) \
+    if (NP == NPV && m == MMV) return tc_active_clusters<NPV, MMV>(M);
+#define AMICA_TC_OCC_NP(NPV) \
+    AMICA_TC_OCC(NPV, 1) AMICA_TC_OCC(NPV, 2) AMICA_TC_OCC(NPV, 3) AMICA_TC_OCC(NPV, 4) \
+    AMICA_TC_OCC(NPV, 5)
+    AMICA_TC_OCC_NP(32)
+    AMICA_TC_OCC_NP(64)
+    AMICA_TC_OCC_NP(128)
+#undef AMICA_TC_OCC_NP
+#undef AMICA_TC_OCC
+    return -1;
+}
+
+cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStream_t st) {
+    if (NP != tc_np(a.n)) return cudaErrorInvalidValue;
+#define AMICA_TC_CASE(NPV, MMV) \
+    if (NP == NPV && a.m == MMV) return launch_tc<NPV, MMV>(a, nclusters, st);
+#define AMICA_TC_NP(NPV) \
+    AMICA_TC_CASE(NPV, 1) AMICA_TC_CASE(NPV, 2) AMICA_TC_CASE(NPV, 3) AMICA_TC_CASE(NPV, 4) \
+    AMICA_TC_CASE(NPV, 5)
+    AMICA_TC_NP(32)
+    AMICA_TC_NP(64)
+    AMICA_TC_NP(128)
+#undef AMICA_TC_NP
+#undef AMICA_TC_CASE
+    return cudaErrorInvalidValue;
+}
 
 }  // namespace amica

@@ -151,6 +151,243 @@ __global__ void __launch_bounds__(kT) k_prep(
 }
 
 // ---------------------------------------------------------------------------
+// k_inverse_smem: W_h = A_h^{-1} by in-place Gauss-Jordan with partial pivoting,
+// the whole n x n FP64 matrix resident in shared memory (n <= 128), one CTA of
+// 1024 threads per model; ldet_h = -sum log|pivot|.  Replaces pinv() and the
+// LU log-determinant (src/amica.cu:27-127, :864-924).
+__global__ void __launch_bounds__(1024) k_inverse_smem(const double* __restrict__ A,
+                                                       const double* __restrict__ gm, double ldetS,
+                                                       double* __restrict__ W,
+                                                       double* __restrict__ ldet,
+                                                       double* __restrict__ ltc64, int n, int* err) {
+    extern __shared__ double gj[];                       // [n][n] row-major, then fcol[n]
+    double* fcol = gj + n * n;
+    __shared__ int perm[128];
+    __shared__ double wb[32];
+    __shared__ int wi[32];
+    __shared__ double piv_s, logdet_s;
+    __shared__ int p_s, bad_s;
+    const int h = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+    const double* Ah = A + (size_t)h * n * n;
+    for (int e = tid; e < n * n; e += nt) {
+        const int r = e / n, c = e % n;
+        gj[e] = Ah[(size_t)c * n + r];
+    }
+    if (tid == 0) { logdet_s = 0.0; bad_s = 0; }
+    __syncthreads();
+    for (int k = 0; k < n; k++) {
+        // pivot row: argmax_{r >= k} |a(r,k)|, lowest index on ties
+        double best = -1.0;
+        int bi = k;
+        for (int r = k + tid; r < n; r += nt) {
+            const double v = fabs(gj[r * n + k]);
+            if (v > best) { best = v; bi = r; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+        }
+        if ((tid & 31) == 0) { wb[tid >> 5] = best; wi[tid >> 5] = bi; }
+        __syncthreads();
+        if (tid == 0) {
+            double b = wb[0];
+            int i = wi[0];
+            for (int w = 1; w < nt / 32; w++)
+                if (wb[w] > b || (wb[w] == b && wi[w] < i)) { b = wb[w]; i = wi[w]; }
+            p_s = i;
+            perm[k] = i;
+        }
+        __syncthreads();
+        const int p = p_s;
+        if (p != k)
+            for (int c = tid; c < n; c += nt) {
+                const double t = gj[k * n + c];
+                gj[k * n + c] = gj[p * n + c];
+                gj[p * n + c] = t;
+            }
+        __syncthreads();
+        if (tid == 0) {
+            piv_s = gj[k * n + k];
+            if (piv_s == 0.0) bad_s = 1;
+            else logdet_s += log(fabs(piv_s));
+        }
+        for (int r = tid; r < n; r += nt) fcol[r] = gj[r * n + k];
+        __syncthreads();
+        if (bad_s) break;
+        const double inv = 1.0 / piv_s;
+        for (int c = tid; c < n; c += nt) gj[k * n + c] = (c == k ? 1.0 : gj[k * n + c]) * inv;
+        __syncthreads();
+        for (int e = tid; e < n * n; e += nt) {
+            const int r = e / n, c = e % n;
+            if (r != k) gj[e] = (c == k ? 0.0 : gj[e]) - fcol[r] * gj[k * n + c];
+        }
+        __syncthreads();
+    }
+    if (bad_s) {
+        if (tid == 0) atomicOr(err, kErrSingular);
+        return;
+    }
+    // undo the row interchanges as column interchanges, last first
+    for (int k = n - 1; k >= 0; k--) {
+        const int p = perm[k];
+        if (p != k)
+            for (int r = tid; r < n; r += nt) {
+                const double t = gj[r * n + k];
+                gj[r * n + k] = gj[r * n + p];
+                gj[r * n + p] = t;
+            }
+        __syncthreads();
+    }
+    double* Wh = W + (size_t)h * n * n;
+    for (int e = tid; e < n * n; e += nt) {
+        const int r = e % n, c = e / n;
+        Wh[e] = gj[r * n + c];                          // column-major W(r, c)
+    }
+    if (tid == 0) {
+        ldet[h] = -logdet_s;
+        ltc64[h] = log(gm[h]) - logdet_s + ldetS;       // src/amica.cu:1009
+    }
+}
+
+// FP32 E-step constants from W and the parameters (grid: models x channel blocks).
+__global__ void __launch_bounds__(128) k_derive(
+    const double* __restrict__ W, const double* __restrict__ c, const double* __restrict__ alpha,
+    const double* __restrict__ mu, const double* __restrict__ beta, const double* __restrict__ rho,
+    float* __restrict__ Wf, float* __restrict__ wcf, MixParam* __restrict__ mp, int n, int m,
+    int NP) {
+    const int h = blockIdx.x;
+    const int i = blockIdx.y * blockDim.x + threadIdx.x;   // channel
+    if (i >= NP) return;
+    const double* Wh = W + (size_t)h * n * n;
+    float* Wfh = Wf + (size_t)h * NP * NP;
+    for (int k = 0; k < NP; k++) Wfh[(size_t)i * NP + k] = (i < n && k < n) ? (float)Wh[(size_t)k * n + i] : 0.f;
+    double wc = 0.0;
+    if (i < n)
+        for (int k = 0; k < n; k++) wc += Wh[(size_t)k * n + i] * c[(size_t)h * n + k];
+    wcf[(size_t)h * NP + i] = (float)wc;
+    for (int j = 0; j < m; j++) {
+        MixParam q;
+        if (i < n) {
+            const size_t idx = ((size_t)h * m + j) * n + i;
+            const double s = sqrt(beta[idx]);
+            const double r = rho[idx];
+            q.s = (float)s;
+            q.off = (float)(s * (mu[idx] + wc));
+            q.cl2 = (float)((log(alpha[idx]) + 0.5 * log(beta[idx]) - M_LN2 - lgamma(1.0 + 1.0 / r)) *
+                            1.4426950408889634);
+            q.rho = (float)r;
+        } else {
+            q.s = 0.f; q.off = 0.f; q.cl2 = 0.f; q.rho = 1.f;
+        }
+        mp[((size_t)h * m + j) * NP + i] = q;
+    }
+}
+
+// Batched FP64 32x32-tiled products on n x n column-major matrices, one
+// (tile, model) per CTA of 256 threads:
+//   kind 0 (A update, src/amica.cu:2330-2342):  Out = X + s_h X Y,
+//          s_h = +lrate (Newton) or -lrate (natural gradient)
+//   kind 1 (phi from Psi):  Out = (Psi - gsum c^T) W^T, written into the
+//          statistics vector's phi block
+__global__ void __launch_bounds__(256) k_gemm64(int kind, const double* __restrict__ X,
+                                                size_t strideX, const double* __restrict__ Y,
+                                                size_t strideY, double* __restrict__ Out,
+                                                size_t strideOut, const double* __restrict__ gs,
+                                                size_t strideG, const double* __restrict__ c,
+                                                const int* __restrict__ use_newton,
+                                                const Ctrl* __restrict__ ctrl, int n) {
+    __shared__ double xs[32][33], ys[32][33];
+    const int h = blockIdx.z;
+    const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+    const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;   // ty: 0..7
+    const double* Xh = X + strideX * h;
+    const double* Yh = Y + strideY * h;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int k0 = 0; k0 < n; k0 += 32) {
+        for (int q = 0; q < 4; q++) {
+            const int rr = ty + 8 * q;                 // tile-local k (for X) / k (for Y)
+            // X(r0 + tx, k0 + rr)
+            const int r = r0 + tx, k = k0 + rr;
+            double xv = 0.0;
+            if (r < n && k < n) {
+                xv = Xh[(size_t)k * n + r];
+                if (kind == 1) xv -= gs[strideG * h + r] * c[(size_t)h * n + k];
+            }
+            xs[tx][rr] = xv;
+            // Y(k0 + rr, c0 + tx): kind 0 -> Y col-major; kind 1 -> W^T(k, col) = W(col, k)
+            const int col = c0 + tx;
+            double yv = 0.0;
+            if (k < n && col < n) yv = (kind == 0) ? Yh[(size_t)col * n + k] : Yh[(size_t)k * n + col];
+            ys[rr][tx] = yv;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int kk = 0; kk < 32; kk++) {
+            const double xv = xs[tx][kk];
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[q] += xv * ys[kk][ty + 8 * q];
+        }
+        __syncthreads();
+    }
+    const int r = r0 + tx;
+    if (r >= n) return;
+    double s = 1.0;
+    if (kind == 0) s = use_newton[h] ? ctrl->lrate : -ctrl->lrate;
+    for (int q = 0; q < 4; q++) {
+        const int col = c0 + ty + 8 * q;
+        if (col >= n) continue;
+        double* o = Out + strideOut * h + (size_t)col * n + r;
+        if (kind == 0) *o = Xh[(size_t)col * n + r] + s * acc[q];
+        else *o = acc[q];
+    }
+}
+
+// Reparametrisation and c update after the A update (src/amica.cu:2367-2512):
+// unit columns of A, mu *= norm, beta /= norm^2, mu -= W_old (cnew - c), c = cnew.
+__global__ void __launch_bounds__(256) k_reparm(int update_A, int do_reparm, double* A,
+                                                const double* __restrict__ Anew,
+                                                const double* __restrict__ W, double* c,
+                                                double* mu, double* beta,
+                                                const double* __restrict__ work, int n, int m) {
+    const int h = blockIdx.x, tid = threadIdx.x;
+    const double* cnew = work + (size_t)h * 4 * n + 3 * n;
+    double* ch = c + (size_t)h * n;
+    __shared__ double norms[256];
+    __shared__ double shift[256];
+    if (update_A) {
+        double* Ah = A + (size_t)h * n * n;
+        const double* An = Anew + (size_t)h * n * n;
+        if (do_reparm) {
+            for (int cc = tid; cc < n; cc += blockDim.x) {
+                double s = 0.0;
+                for (int r = 0; r < n; r++) s += An[(size_t)cc * n + r] * An[(size_t)cc * n + r];
+                norms[cc] = sqrt(s);
+            }
+            const double* Wh = W + (size_t)h * n * n;
+            for (int i = tid; i < n; i += blockDim.x) {
+                double acc = 0.0;
+                for (int k = 0; k < n; k++) acc += Wh[(size_t)k * n + i] * (cnew[k] - ch[k]);
+                shift[i] = acc;
+            }
+            __syncthreads();
+            for (int e = tid; e < n * n; e += blockDim.x) Ah[e] = An[e] / norms[e / n];
+            for (int e = tid; e < m * n; e += blockDim.x) {
+                const int i = e % n;
+                const size_t idx = (size_t)h * m * n + e;
+                mu[idx] *= norms[i];
+                beta[idx] /= (norms[i] * norms[i]);
+                mu[idx] -= shift[i];
+            }
+        } else {
+            for (int e = tid; e < n * n; e += blockDim.x) Ah[e] = An[e];
+        }
+        __syncthreads();
+    }
+    for (int i = tid; i < n; i += blockDim.x) ch[i] = cnew[i];   // src/amica.cu:2456-2462
+}
+
+// ---------------------------------------------------------------------------
 // k_reduce: raw[h][e] = sum over clusters of partial[q][h][e], fixed order.
 // Replaces the block/device reductions of src/amica.cu:1618-1920.
 __global__ void k_reduce(const double* __restrict__ partial, double* __restrict__ raw, int nclusters,
@@ -169,10 +406,11 @@ __global__ void k_reduce(const double* __restrict__ partial, double* __restrict_
 // phi = (Psi - gsum c^T) W^T, and the per-block factors of src/kernels.cu:616
 // (kappa * beta), :745 (mu_denom * sqrt(beta)), :748-750 (rho * beta_denom).
 __global__ void __launch_bounds__(kT) k_finalize(
-    const double* __restrict__ raw, const double* __restrict__ W, const double* __restrict__ c,
+    const double* __restrict__ raw, const double* __restrict__ W, const double* __restrict__ A,
+    const double* __restrict__ c,
     const double* __restrict__ beta, const double* __restrict__ rho,
     const double* __restrict__ ltc64, const Ctrl* __restrict__ ctrl, double* __restrict__ stats,
-    int n, int m) {
+    int n, int m, int psi_is_phi) {
     const int h = blockIdx.x, tid = threadIdx.x;
     PartLayout PL{n, m};
     StatLayout SL{n, m};
@@ -180,8 +418,12 @@ __global__ void __launch_bounds__(kT) k_finalize(
     double* S = stats + SL.base(h);
     if (h == 0 && tid == 0) stats[0] = R[0] + (double)ctrl->nkeep * ltc64[0];
     if (tid == 0) S[SL.vs()] = R[1];
+    const double* Ah = A + (size_t)h * n * n;
     for (int i = tid; i < n; i += kT) {
-        S[SL.cn() + i] = R[PL.cn() + i];
+        // sum_t v x_i = (A sum_t v b)_i + vsum c_i, since x - c = A b
+        double acc = R[1] * c[(size_t)h * n + i];
+        for (int k = 0; k < n; k++) acc += Ah[(size_t)k * n + i] * R[PL.cn() + k];
+        S[SL.cn() + i] = acc;
         S[SL.s2() + i] = R[PL.s2() + i];
     }
     const double* Psi = R + PL.psi();
@@ -190,10 +432,7 @@ __global__ void __launch_bounds__(kT) k_finalize(
     const double* ch = c + (size_t)h * n;
     for (int e = tid; e < n * n; e += kT) {
         const int i = e % n, k = e / n;
-        double acc = 0.0;
-        for (int l = 0; l < n; l++)
-            acc += (Psi[(size_t)l * n + i] - gs[i] * ch[l]) * Wh[(size_t)l * n + k];
-        S[SL.phi() + (size_t)k * n + i] = acc;
+        if (psi_is_phi) S[SL.phi() + (size_t)k * n + i] = Psi[e];
     }
     for (int e = tid; e < m * n; e += kT) {
         const size_t idx = (size_t)h * m * n + e;
@@ -527,20 +766,38 @@ static MCfg to_mcfg(const MStepCfgHost& h) {
 }
 
 cudaError_t launch_prep(const MStepBuffers& b, const MStepCfgHost& h, cudaStream_t st) {
-    k_prep<<<h.M, kT, 0, st>>>(b.A, b.c, b.alpha, b.mu, b.beta, b.rho, b.gm, h.ldetS, b.aug, b.W,
-                               b.ldet, b.ltc64, b.Wf, b.wcf, b.mp, h.n, h.m, h.NP, b.err);
+    if (h.n <= 128) {
+        const size_t smem = sizeof(double) * ((size_t)h.n * h.n + h.n);
+        cudaError_t e = cudaFuncSetAttribute(k_inverse_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        k_inverse_smem<<<h.M, 1024, smem, st>>>(b.A, b.gm, h.ldetS, b.W, b.ldet, b.ltc64, h.n, b.err);
+        dim3 grid(h.M, (h.NP + 127) / 128);
+        k_derive<<<grid, 128, 0, st>>>(b.W, b.c, b.alpha, b.mu, b.beta, b.rho, b.Wf, b.wcf, b.mp, h.n,
+                                       h.m, h.NP);
+    } else {
+        k_prep<<<h.M, kT, 0, st>>>(b.A, b.c, b.alpha, b.mu, b.beta, b.rho, b.gm, h.ldetS, b.aug, b.W,
+                                   b.ldet, b.ltc64, b.Wf, b.wcf, b.mp, h.n, h.m, h.NP, b.err);
+    }
     return cudaGetLastError();
 }
 
 cudaError_t launch_reduce_finalize(const MStepBuffers& b, const MStepCfgHost& h, int nclusters,
                                    cudaStream_t st) {
     PartLayout PL{h.n, h.m};
+    StatLayout SL{h.n, h.m};
     const int64_t total = (int64_t)h.M * PL.stride();
     int grid = (int)((total + 255) / 256);
     if (grid > 4096) grid = 4096;
     k_reduce<<<grid, 256, 0, st>>>(b.partial, b.raw, nclusters, h.M, PL.stride());
-    k_finalize<<<h.M, kT, 0, st>>>(b.raw, b.W, b.c, b.beta, b.rho, b.ltc64, b.ctrl, b.stats, h.n,
-                                   h.m);
+    k_finalize<<<h.M, kT, 0, st>>>(b.raw, b.W, b.A, b.c, b.beta, b.rho, b.ltc64, b.ctrl, b.stats,
+                                   h.n, h.m, h.psi_is_phi);
+    if (!h.psi_is_phi) {
+        dim3 g((h.n + 31) / 32, (h.n + 31) / 32, h.M);
+        k_gemm64<<<g, 256, 0, st>>>(1, b.raw + PL.psi(), PL.stride(), b.W, (size_t)h.n * h.n,
+                                    b.stats + SL.base(0) + SL.phi(), SL.S(), b.raw + PL.gs(),
+                                    PL.stride(), b.c, nullptr, nullptr, h.n);
+    }
     return cudaGetLastError();
 }
 
@@ -550,8 +807,13 @@ cudaError_t launch_mstep(const MStepBuffers& b, const MStepCfgHost& h, const flo
     k_mstep_params<<<h.M, kT, 0, st>>>(cf, b.stats, b.ctrl, b.gm, b.alpha, b.mu, b.beta, b.rho,
                                        b.work, b.B, b.bflag, b.use_newton);
     k_ctrl<<<1, 32, 0, st>>>(cf, b.stats, b.ctrl, b.bflag, b.hist, b.hist_cap);
-    k_mstep_A<<<h.M, kT, 0, st>>>(cf, b.ctrl, b.A, b.Anew, b.B, b.use_newton, b.W, b.c, b.mu,
-                                  b.beta, b.work);
+    if (h.update_A) {
+        dim3 g((h.n + 31) / 32, (h.n + 31) / 32, h.M);
+        k_gemm64<<<g, 256, 0, st>>>(0, b.A, (size_t)h.n * h.n, b.B, (size_t)h.n * h.n, b.Anew,
+                                    (size_t)h.n * h.n, nullptr, 0, nullptr, b.use_newton, b.ctrl, h.n);
+    }
+    k_reparm<<<h.M, 256, 0, st>>>(h.update_A, h.do_reparm, b.A, b.Anew, b.W, b.c, b.mu, b.beta,
+                                  b.work, h.n, h.m);
     if (h.do_reject && P_rel && keep)
         k_reject<<<1, kT, 0, st>>>(cf, b.ctrl, P_rel, keep, T, b.chunk, b.hist, b.hist_cap, 0);
     return cudaGetLastError();

@@ -259,10 +259,19 @@ __global__ void k_var(const float* __restrict__ x, int64_t T, int n, const doubl
 
 // x_out[t][i] = sum_k S(i,k) (x[t][k] - mean[k]) in FP64, rounded to FP32;
 // padded channels are zero.
+// Round to the TF32 grid, nearest with ties away from zero (the tensor cores
+// read only the top 19 bits of an FP32 operand, i.e. truncate; storing the data
+// pre-rounded makes the TF32 contraction see an unbiased value).
+__device__ __forceinline__ float round_tf32(float v) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+    return __uint_as_float(r);
+}
+
 __global__ void __launch_bounds__(256) k_apply_sphere(const float* __restrict__ x, int64_t T, int n,
                                                       const double* __restrict__ mean,
                                                       const double* __restrict__ S,
-                                                      float* __restrict__ xo, int ldx) {
+                                                      float* __restrict__ xo, int ldx, int tf32) {
     extern __shared__ double xc[];   // [16][n]
     const int64_t t0 = (int64_t)blockIdx.x * 16;
     for (int e = threadIdx.x; e < 16 * n; e += blockDim.x) {
@@ -278,18 +287,19 @@ __global__ void __launch_bounds__(256) k_apply_sphere(const float* __restrict__ 
         double acc = 0.0;
         if (i < n)
             for (int k = 0; k < n; k++) acc += S[(size_t)k * n + i] * xc[r * n + k];
-        xo[t * ldx + i] = (float)acc;
+        xo[t * ldx + i] = tf32 ? round_tf32((float)acc) : (float)acc;
     }
 }
 
 __global__ void k_convert(const double* __restrict__ xs, int64_t T, int n, float* __restrict__ xo,
-                          int ldx) {
+                          int ldx, int tf32) {
     const int64_t total = T * (int64_t)ldx;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
          e += (int64_t)gridDim.x * blockDim.x) {
         const int64_t t = e / ldx;
         const int i = (int)(e % ldx);
-        xo[e] = (i < n) ? (float)xs[t * n + i] : 0.f;
+        const float v = (i < n) ? (float)xs[t * n + i] : 0.f;
+        xo[e] = tf32 ? round_tf32(v) : v;
     }
 }
 
@@ -300,7 +310,7 @@ namespace amica {
 // evwork: >= 4 n^2 + 4 n doubles
 cudaError_t launch_preprocess(const float* raw, int64_t T, int n, int do_sphere, double* means,
                               double* cov, double* sphere, double* evwork, double* ldetS_dev,
-                              float* x, int ldx, cudaStream_t st) {
+                              float* x, int ldx, int tf32, cudaStream_t st) {
     if (n > 256) return cudaErrorInvalidValue;
     const int nblk = (int)((T + kChunk - 1) / kChunk);
     double* part = nullptr;
@@ -332,14 +342,14 @@ cudaError_t launch_preprocess(const float* raw, int64_t T, int n, int do_sphere,
     const size_t smem2 = sizeof(double) * 16 * n;
     e = cudaFuncSetAttribute(k_apply_sphere, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);
     if (e != cudaSuccess) { cudaFreeAsync(part, st); return e; }
-    k_apply_sphere<<<(unsigned)((T + 15) / 16), 256, smem2, st>>>(raw, T, n, means, sphere, x, ldx);
+    k_apply_sphere<<<(unsigned)((T + 15) / 16), 256, smem2, st>>>(raw, T, n, means, sphere, x, ldx, tf32);
     cudaFreeAsync(part, st);
     return cudaGetLastError();
 }
 
-cudaError_t launch_convert_sphered(const double* xs, int64_t T, int n, float* x, int ldx,
+cudaError_t launch_convert_sphered(const double* xs, int64_t T, int n, float* x, int ldx, int tf32,
                                    cudaStream_t st) {
-    k_convert<<<2048, 256, 0, st>>>(xs, T, n, x, ldx);
+    k_convert<<<2048, 256, 0, st>>>(xs, T, n, x, ldx, tf32);
     return cudaGetLastError();
 }
 

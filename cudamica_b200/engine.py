@@ -41,7 +41,7 @@ EXPORTED = (
     "amica_stats_len", "amica_get_loglik", "amica_loglik_adjoint", "amica_reject_now",
     "amica_write_outputs", "amica_status_string", "amica_kernel_name", "amica_get_p_relative",
     "amica_last_cuda_error", "amica_set_iter_state", "amica_get_sphere", "amica_time_estep",
-    "amica_launches_per_iteration")
+    "amica_launches_per_iteration", "amica_selftest_umma")
 
 
 class Cfg(C.Structure):
@@ -106,6 +106,7 @@ def lib():
         L.amica_time_estep.argtypes = [vp, _i64, _pd, C.POINTER(_i64)]
         L.amica_launches_per_iteration.restype = _i64
         L.amica_launches_per_iteration.argtypes = [vp]
+        L.amica_selftest_umma.argtypes = [C.c_int, C.c_int, C.c_int, _pf, _pf, _pf, C.POINTER(C.c_int)]
         _lib = L
     return _lib
 
@@ -125,6 +126,21 @@ def default_cfg(**over) -> Cfg:
     for k, v in over.items():
         setattr(c, k, v)
     return c
+
+
+def selftest_umma(mode: int, A: np.ndarray, B: np.ndarray) -> np.ndarray:
+    """Run one tensor-core contraction with the E-step's layouts (see header)."""
+    A = np.ascontiguousarray(A, dtype=np.float32)
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    K = A.shape[1]
+    N = B.shape[0]
+    D = np.empty((128, N), dtype=np.float32)
+    derr = C.c_int(0)
+    _chk(lib().amica_selftest_umma(mode, N, K, A.ctypes.data_as(_pf), B.ctypes.data_as(_pf),
+                                   D.ctypes.data_as(_pf), C.byref(derr)), "amica_selftest_umma")
+    if derr.value:
+        raise AmicaError(-24, "amica_selftest_umma (device wait)")
+    return D
 
 
 class Amica:

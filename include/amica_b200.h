@@ -181,6 +181,14 @@ int amica_time_estep(amica_ctx *ctx, int64_t reps, double *ms_per_launch, int64_
 /* Number of kernels one EM iteration launches. */
 int64_t amica_launches_per_iteration(amica_ctx *ctx);
 
+/* Self-test of the tensor-core contraction forms used by the mixed-precision
+ * E-step (one CTA, host buffers): D = A B^T with A (128 x K) and B (N x K),
+ * B K-major in shared memory; mode 0: A in shared memory, mode 1: A in tensor
+ * memory, mode 2: A split into TF32 hi (shared) + lo (tensor memory) halves.
+ * K in {16, 32, 48, 64}, N a multiple of 16 up to 64.  D is 128 x N float. */
+int amica_selftest_umma(int mode, int N, int K, const float *A, const float *B, float *D,
+                        int *device_err);
+
 /* Last CUDA runtime error code seen by any call (0 = none). */
 int amica_last_cuda_error(void);
 

