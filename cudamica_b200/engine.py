@@ -41,7 +41,7 @@ EXPORTED = (
     "amica_stats_len", "amica_get_loglik", "amica_loglik_adjoint", "amica_reject_now",
     "amica_write_outputs", "amica_status_string", "amica_kernel_name", "amica_get_p_relative",
     "amica_last_cuda_error", "amica_set_iter_state", "amica_get_sphere", "amica_time_estep",
-    "amica_launches_per_iteration", "amica_selftest_umma")
+    "amica_launches_per_iteration", "amica_selftest_umma", "amica_estep_stats_noalloc")
 
 
 class Cfg(C.Structure):
@@ -107,6 +107,8 @@ def lib():
         L.amica_launches_per_iteration.restype = _i64
         L.amica_launches_per_iteration.argtypes = [vp]
         L.amica_selftest_umma.argtypes = [C.c_int, C.c_int, C.c_int, _pf, _pf, _pf, C.POINTER(C.c_int)]
+        L.amica_estep_stats_noalloc.argtypes = [vp, _i64, _i64, _i64, _i64, _i64, vp, vp, vp, vp,
+                                                vp, vp, vp, _dbl, vp, _i64, _i64, vp, vp]
         _lib = L
     return _lib
 
@@ -141,6 +143,20 @@ def selftest_umma(mode: int, A: np.ndarray, B: np.ndarray) -> np.ndarray:
     if derr.value:
         raise AmicaError(-24, "amica_selftest_umma (device wait)")
     return D
+
+
+def estep_stats_noalloc(x_ptr: int, ldx: int, n: int, T: int, M: int, m: int, A_ptr: int,
+                        c_ptr: int, alpha_ptr: int, mu_ptr: int, beta_ptr: int, rho_ptr: int,
+                        gm_ptr: int, ldetS: float, stats_ptr: int, keep_ptr: int = 0,
+                        nkeep: int | None = None, update_rho: int = 1, stream: int = 0) -> None:
+    """The allocation-free E-step statistics call; every pointer is a device
+    address owned by the caller (see include/amica_b200.h)."""
+    rc = lib().amica_estep_stats_noalloc(
+        C.c_void_p(x_ptr), ldx, n, T, M, m, C.c_void_p(A_ptr), C.c_void_p(c_ptr),
+        C.c_void_p(alpha_ptr), C.c_void_p(mu_ptr), C.c_void_p(beta_ptr), C.c_void_p(rho_ptr),
+        C.c_void_p(gm_ptr), float(ldetS), C.c_void_p(keep_ptr or None), T if nkeep is None else nkeep,
+        update_rho, C.c_void_p(stats_ptr), C.c_void_p(stream or None))
+    _chk(rc, "amica_estep_stats_noalloc")
 
 
 class Amica:

@@ -189,6 +189,28 @@ int64_t amica_launches_per_iteration(amica_ctx *ctx);
 int amica_selftest_umma(int mode, int N, int K, const float *A, const float *B, float *D,
                         int *device_err);
 
+/* E-step sufficient statistics with no allocation at all, for callers that
+ * cannot call cudaMalloc (code running inside another framework's memory pool,
+ * or a process that forbids device allocations after start-up).  No
+ * counterpart in the reference: its EM loop allocates per-block buffers.
+ * All pointers are DEVICE memory owned by the caller: x is T x ldx float32
+ * sphered data with ldx the channel count padded to 32, 64 or 128 (padding
+ * channels zero); A (M x n x n), c, alpha, mu, beta, rho, gm as in
+ * amica_set_params(); keep (T bytes) may be NULL with nkeep = T; stats
+ * receives amica_stats_len(n, M, m) doubles.  Intermediate data lives in a
+ * fixed 5 MiB device array inside this library (held by every GPU that loads
+ * it until exit); shapes needing more (roughly n = 128 with M > 3) return
+ * AMICA_ERR_UNSUPPORTED.  The first call on a device resolves that array's
+ * address for the device, so make it before any stream capture.  Calls share
+ * the array: calls whose GPU work overlaps race, so serialise them.  The call
+ * enqueues on `stream` (a cudaStream_t, NULL = default) and returns after
+ * synchronising it. */
+int amica_estep_stats_noalloc(const float *x, int64_t ldx, int64_t n, int64_t T, int64_t M,
+                              int64_t m, const double *A, const double *c, const double *alpha,
+                              const double *mu, const double *beta, const double *rho,
+                              const double *gm, double ldetS, const uint8_t *keep, int64_t nkeep,
+                              int64_t update_rho, double *stats, void *stream);
+
 /* Last CUDA runtime error code seen by any call (0 = none). */
 int amica_last_cuda_error(void);
 
