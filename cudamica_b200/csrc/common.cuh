@@ -95,8 +95,8 @@ struct EStepArgs {
 
 // Device buffers and host-side settings of the FP64 M-step kernels.
 struct MStepBuffers {
-    double *A, *Anew, *c, *alpha, *mu, *beta, *rho, *gm, *W, *ldet, *ltc64, *aug;
-    double *partial, *raw, *stats, *work, *B, *chunk;
+    double *A, *Anew, *c, *alpha, *mu, *beta, *rho, *gm, *W, *ldet, *ltc64;
+    double *partial, *raw, *stats, *work, *chunk;
     int64_t* bflag;
     int* use_newton;
     float *Wf, *wcf;
@@ -113,6 +113,7 @@ struct MStepCfgHost {
     int do_reject, rejstart, rejint, maxrej;
     double lratemax, lnatrate, lratefact, rholrate, rhomin, rhomax, rejsig, ldetS;
     int psi_is_phi;   // 1: the E-step's n x n slot already holds phi = sum g b^T (tensor-core form)
+    int psi_step;     // only every psi_step-th partial slot carries the n x n block
 };
 
 }  // namespace amica

@@ -2,10 +2,11 @@
 // pipeline and the C ABI declared in include/amica_b200.h.
 //
 // One iteration is a fixed sequence of kernels on the context's stream:
-//   k_prep (FP64 inverse, log-det, E-step constants)
+//   k_inverse_derive (FP64 inverse, log-det, E-step constants)
 //   -> fused E-step (plain FP32 or tcgen05 TF32)
 //   -> k_reduce + k_finalize (deterministic FP64 reduction of per-CTA sums)
-//   -> k_mstep_params -> k_ctrl -> k_mstep_A (-> k_reject on schedule)
+//   -> k_mstep_params -> k_ctrl -> k_gemm64 (A update) -> k_reparm
+//   (-> k_reject on schedule)
 // with no host synchronisation, so amica_run() replays one captured CUDA graph
 // per iteration.  This replaces runamica()'s iteration body
 // (src/amica.cu:820-2541), which synchronised with the host ~T/block_size
@@ -176,9 +177,12 @@ int enqueue_estep(amica_ctx* c) {
     return AMICA_OK;
 }
 
-// Kernels one iteration launches: prep, E-step, reduce, finalize, params, ctrl,
-// A update (+ rejection when enabled).
-int launches_per_iteration(const amica_ctx* c) { return 7 + (c->hc.do_reject ? 1 : 0); }
+// Kernels one iteration launches: inverse/derive, E-step, reduce, finalize
+// (+ phi from Psi in the plain form), params, ctrl, A update (when A is
+// updated), reparametrisation (+ rejection when enabled).
+int launches_per_iteration(const amica_ctx* c) {
+    return 7 + (c->hc.psi_is_phi ? 0 : 1) + (c->hc.update_A ? 1 : 0) + (c->hc.do_reject ? 1 : 0);
+}
 
 int enqueue_iteration(amica_ctx* c) {
     TRY(enqueue_estep(c));
@@ -328,6 +332,7 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     h.rholrate = cfg->rholrate; h.rhomin = cfg->rhomin; h.rhomax = cfg->rhomax;
     h.rejsig = cfg->rejsig; h.ldetS = 0.0;
     h.psi_is_phi = c->use_tc ? 1 : 0;
+    h.psi_step = c->use_tc ? tc_partial_groups() : 1;
 
     MStepBuffers& b = c->b;
     const size_t nn = (size_t)n * n, mn = (size_t)m * n;
@@ -335,13 +340,13 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
 #define AL(p, cnt) if ((r = dalloc(&(p), (cnt))) != AMICA_OK) { amica_destroy(c); return r; }
     AL(b.A, M * nn); AL(b.Anew, M * nn); AL(b.c, M * n); AL(b.alpha, M * mn); AL(b.mu, M * mn);
     AL(b.beta, M * mn); AL(b.rho, M * mn); AL(b.gm, M); AL(b.W, M * nn); AL(b.ldet, M);
-    AL(b.ltc64, M); AL(b.aug, M * nn * 2);
+    AL(b.ltc64, M);
     PartLayout PL{(int)n, (int)m};
     c->nslots = c->nclusters * (c->use_tc ? tc_partial_groups() : 1);
     AL(b.partial, (size_t)c->nslots * M * PL.stride());
     AL(b.raw, M * (size_t)PL.stride());
     AL(b.stats, (size_t)amica_stats_len(n, M, m));
-    AL(b.work, M * 4 * n); AL(b.B, M * nn);
+    AL(b.work, M * 4 * n);
     const int64_t nch = (T + 4095) / 4096;
     AL(b.chunk, 2 * nch + 2);
     AL(b.bflag, M); AL(b.use_newton, M);
@@ -372,8 +377,8 @@ int amica_destroy(amica_ctx* c) {
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     void* ptrs[] = {c->b.A, c->b.Anew, c->b.c, c->b.alpha, c->b.mu, c->b.beta, c->b.rho, c->b.gm,
-                    c->b.W, c->b.ldet, c->b.ltc64, c->b.aug, c->b.partial, c->b.raw, c->b.stats,
-                    c->b.work, c->b.B, c->b.chunk, c->b.bflag, c->b.use_newton, c->b.Wf, c->b.wcf,
+                    c->b.W, c->b.ldet, c->b.ltc64, c->b.partial, c->b.raw, c->b.stats,
+                    c->b.work, c->b.chunk, c->b.bflag, c->b.use_newton, c->b.Wf, c->b.wcf,
                     c->b.mp, c->b.ctrl, c->b.hist, c->b.err, c->d_keep, c->d_Lt, c->d_P, c->d_x,
                     c->d_rawx, c->d_means, c->d_sphere, c->d_cov, c->d_evwork, c->d_ldetS,
                     c->d_backup, c->d_gradp, c->d_grad};

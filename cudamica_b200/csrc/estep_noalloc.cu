@@ -124,6 +124,7 @@ extern "C" int amica_estep_stats_noalloc(const float* x, int64_t ldx, int64_t n,
     h.n = (int)n; h.m = (int)m; h.M = (int)M; h.NP = NP;
     h.ldetS = ldetS;
     h.psi_is_phi = 0;
+    h.psi_step = 1;
     cudaStream_t st = (cudaStream_t)stream;
 
     // the only state that must start from zero each call: the error flag

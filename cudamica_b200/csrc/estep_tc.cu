@@ -104,6 +104,12 @@ __device__ __forceinline__ uint32_t mapa(uint32_t addr, uint32_t rank) {
 __device__ __forceinline__ void st_cluster_f32(uint32_t addr, float v) {
     asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(addr), "f"(v) : "memory");
 }
+// Asynchronous 4-byte store into a cluster peer's shared memory; completion is
+// counted on that peer's mbarrier as transaction bytes (no fence needed).
+__device__ __forceinline__ void st_async_f32(uint32_t addr, float v, uint32_t bar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f32 [%0], %1, [%2];"
+                 ::"r"(addr), "f"(v), "r"(bar) : "memory");
+}
 __device__ __forceinline__ void mbar_arrive_remote(uint32_t addr) {
     asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(addr) : "memory");
 }
@@ -164,7 +170,12 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
           "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
           "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    // the wait names the destination registers so that no use moves above it
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]),
+                   "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]),
+                   "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+                 :: "memory");
 #pragma unroll
     for (int q = 0; q < 16; q++) v[q] = __uint_as_float(r[q]);
 }
@@ -172,10 +183,128 @@ __device__ __forceinline__ void tmem_ld4(uint32_t taddr, float* v) {
     uint32_t r0, r1, r2, r3;
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
                  : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r0), "+r"(r1), "+r"(r2), "+r"(r3) :: "memory");
     v[0] = __uint_as_float(r0); v[1] = __uint_as_float(r1);
     v[2] = __uint_as_float(r2); v[3] = __uint_as_float(r3);
 }
+__device__ __forceinline__ void tmem_st4_nowait(uint32_t taddr, const float* v) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};"
+                 ::"r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])),
+                   "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])) : "memory");
+}
+// Fire-and-forget FP64 add to global memory.  Each address is updated by one
+// thread only, so the adds land in program order and the sum is deterministic.
+__device__ __forceinline__ void red_add_f64(double* p, double v) {
+    asm volatile("red.global.add.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() {
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_ld4_nowait(uint32_t taddr, uint32_t* r) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(taddr));
+}
+// Wait for this thread's tensor-memory loads; r (the destination registers of
+// one of them) is named so that its uses stay after the wait.  A second call
+// for another destination finds nothing pending and only orders its uses.
+__device__ __forceinline__ void tmem_wait_ld(uint32_t* r) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]) :: "memory");
+}
+// Tensor-memory column of chunk c (kSub columns) of the log2|y| cache: the
+// 16-column gaps after the two b buffers when a chunk fits there, then the 128
+// columns after W_lo.
+constexpr int kL2Gap = kSub <= 16 ? 2 : 0;
+constexpr int kL2Chunks = kL2Gap + 128 / kSub;
+__device__ __forceinline__ uint32_t l2_chunk_col(int c) {
+    if (kL2Gap && c < kL2Gap) return c == 0 ? 48u : 112u;
+    return 384u + (uint32_t)(kSub * (c - kL2Gap));
+}
+
+// Mixture math on one float or on a float2 pair of mixtures (sm_100 packed
+// FP32 instructions: one issue for two lanes of work).
+__device__ __forceinline__ float splat_v(float a, float) { return a; }
+__device__ __forceinline__ float2 splat_v(float a, float2) { return make_float2(a, a); }
+__device__ __forceinline__ float vfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float vmul(float a, float b) { return a * b; }
+__device__ __forceinline__ float2 vmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float vadd(float a, float b) { return a + b; }
+__device__ __forceinline__ float2 vadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float vabsmax(float y) { return fmaxf(fabsf(y), kTinyAbs); }
+__device__ __forceinline__ float2 vabsmax(float2 y) { return make_float2(vabsmax(y.x), vabsmax(y.y)); }
+__device__ __forceinline__ float vlg2(float x) { return ptx_lg2(x); }
+__device__ __forceinline__ float2 vlg2(float2 x) { return make_float2(ptx_lg2(x.x), ptx_lg2(x.y)); }
+__device__ __forceinline__ float vex2(float x) { return ptx_ex2(x); }
+__device__ __forceinline__ float2 vex2(float2 x) { return make_float2(ptx_ex2(x.x), ptx_ex2(x.y)); }
+// 1/y with |y| clamped to ay
+__device__ __forceinline__ float vrcp_signed(float ay, float y) { return ptx_rcp(copysignf(ay, y)); }
+__device__ __forceinline__ float2 vrcp_signed(float2 ay, float2 y) {
+    return make_float2(ptx_rcp(copysignf(ay.x, y.x)), ptx_rcp(copysignf(ay.y, y.y)));
+}
+
+// Per-mixture parameters of one channel, as scalars or pairs.
+template <class V>
+struct MixV {
+    V s, npo, pc, pr, sr;   // sqrt(beta), -sqrt(beta)(mu + w c), log2 normaliser, rho, sqrt(beta) rho
+};
+
+// Phase 1 for one sample: q = log2 of the mixture term, and log2|y|.
+template <class V>
+__device__ __forceinline__ V dens_q(const MixV<V>& P, float bx, V& L2) {
+    const V y = vfma(P.s, splat_v(bx, V{}), P.npo);
+    L2 = vlg2(vabsmax(y));
+    const V p = vex2(vmul(P.pr, L2));
+    return vfma(splat_v(-kLog2e, V{}), p, P.pc);
+}
+
+// Phase 2 for one sample: the seven sums A0..A6 and the g term.
+template <class V, bool kHaveL2>
+__device__ __forceinline__ void dens_acc(const MixV<V>& P, float bx, V L2, float nlse, float v, V* A,
+                                         V& g) {
+    const V y = vfma(P.s, splat_v(bx, V{}), P.npo);
+    const V ay = vabsmax(y);
+    if constexpr (!kHaveL2) L2 = vlg2(ay);
+    const V p = vex2(vmul(P.pr, L2));
+    const V z = vex2(vadd(vfma(splat_v(-kLog2e, V{}), p, P.pc), splat_v(nlse, V{})));
+    const V uu = vmul(z, splat_v(v, V{}));
+    const V ri = vrcp_signed(ay, y);
+    const V w = vmul(uu, p);
+    A[0] = vadd(A[0], uu);
+    A[1] = vadd(A[1], w);
+    A[2] = vfma(w, p, A[2]);
+    A[3] = vfma(w, L2, A[3]);
+    const V wr = vmul(w, ri);
+    A[4] = vadd(A[4], wr);
+    const V wr2 = vmul(wr, ri);
+    A[5] = vadd(A[5], wr2);
+    A[6] = vfma(wr2, p, A[6]);
+    g = vfma(P.sr, wr, g);
+}
+
+// log-sum-exp over the mixtures in log2 units: qmax + log2(sum 2^(q - qmax)).
+// The term of the maximum is exactly 1, so for m <= 3 its ex2 is skipped.
+template <int MM>
+__device__ __forceinline__ float lse2(const float* q) {
+    if constexpr (MM == 1) {
+        return q[0];
+    } else if constexpr (MM == 2) {
+        const float mx = fmaxf(q[0], q[1]), mn = fminf(q[0], q[1]);
+        return mx + ptx_lg2(1.f + ptx_ex2(mn - mx));
+    } else if constexpr (MM == 3) {
+        const float m01 = fmaxf(q[0], q[1]), n01 = fminf(q[0], q[1]);
+        const float mx = fmaxf(m01, q[2]), o1 = fminf(m01, q[2]);
+        return mx + ptx_lg2(1.f + ptx_ex2(o1 - mx) + ptx_ex2(n01 - mx));
+    } else {
+        float mx = q[0];
+#pragma unroll
+        for (int j = 1; j < MM; j++) mx = fmaxf(mx, q[j]);
+        float se = 0.f;
+#pragma unroll
+        for (int j = 0; j < MM; j++) se += ptx_ex2(q[j] - mx);
+        return mx + ptx_lg2(se);
+    }
+}
+
 __device__ __forceinline__ float tf32_rna(float x) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
@@ -217,18 +346,20 @@ struct TcShape {
     static constexpr uint32_t OFF_X1 = OFF_X0 + X_BYTES;
     static constexpr uint32_t OFF_G = OFF_X1 + X_BYTES;
     static constexpr uint32_t OFF_BT = OFF_G + G_BYTES;                  // b tile, same layout as G
-    static constexpr uint32_t OFF_RED = OFF_BT + G_BYTES;                // [2][WG][4 warps][16] f32
-    static constexpr uint32_t OFF_SLOT = OFF_RED + 2 * kWG * 4 * 16 * 4;  // [2][8 models][64] f32
-    static constexpr uint32_t OFF_BAR = OFF_SLOT + 2 * kMaxModels * kS * 4;
-    static constexpr uint32_t NBAR = 24;
+    // per-warp channel sums of Lt from every model's CTA: [2][8 models][4 warps][kS] f32
+    static constexpr uint32_t OFF_SLOT = OFF_BT + G_BYTES;
+    static constexpr uint32_t OFF_LSE = OFF_SLOT + 2 * kMaxModels * 4 * kS * 4;  // [WG][kSub][128] f32
+    static constexpr uint32_t OFF_BAR = OFF_LSE + kWG * kSub * 128 * 4;
+    static constexpr uint32_t NBAR = 32;
     static constexpr uint32_t OFF_MISC = OFF_BAR + NBAR * 8;
     static constexpr uint32_t BYTES = OFF_MISC + 64;
-    static constexpr uint32_t TMEM_COLS = 512;   // b: [0,48) [64,112); phi: [128,128+NP); W_lo: [256,256+NP)
+    static constexpr uint32_t TMEM_COLS = 512;   // b: [0,48) [64,112); phi: [128,128+NP); W_lo: [256,256+NP);
+                                                 // log2|y| cache: [48,64) [112,128) [384,512)
 };
 
 enum { BAR_FULL0 = 0, BAR_FULL1, BAR_EMPTY0, BAR_EMPTY1, BAR_BFULL0, BAR_BFULL1, BAR_BEMPTY0,
-       BAR_BEMPTY1, BAR_GFULL, BAR_GEMPTY, BAR_LT0, BAR_LT1, BAR_PSI, BAR_DRAIN,
-       BAR_RED0 /* 2 parities x kWG warpgroups: BAR_RED0 + par * kWG + wg */ };
+       BAR_BEMPTY1, BAR_GFULL, BAR_GEMPTY, BAR_PSI, BAR_DRAIN,
+       BAR_LT0 /* 2 parities x kWG warpgroups: BAR_LT0 + par * kWG + wg */ };
 
 struct TcArgs {
     EStepArgs e;
@@ -245,7 +376,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     float* Wsm = (float*)(sm + Sh::OFF_W);
     float* Gsm = (float*)(sm + Sh::OFF_G);
-    float* red = (float*)(sm + Sh::OFF_RED);
     float* slot = (float*)(sm + Sh::OFF_SLOT);
     uint64_t* bar = (uint64_t*)(sm + Sh::OFF_BAR);
     uint32_t* tmem_holder = (uint32_t*)(sm + Sh::OFF_MISC);
@@ -270,11 +400,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         mbar_init(&bar[BAR_BEMPTY1], kDensWarps);
         mbar_init(&bar[BAR_GFULL], kDensWarps);
         mbar_init(&bar[BAR_GEMPTY], 1);
-        mbar_init(&bar[BAR_LT0], (uint32_t)(16 * kWG * M));
-        mbar_init(&bar[BAR_LT1], (uint32_t)(16 * kWG * M));
+        // one local arrival (with the expected bytes) per tile; the data comes by st.async
+        for (int r = 0; r < 2 * kWG; r++) mbar_init(&bar[BAR_LT0 + r], 1);
         mbar_init(&bar[BAR_PSI], 1);
         mbar_init(&bar[BAR_DRAIN], 1);
-        for (int r = 0; r < 2 * kWG; r++) mbar_init(&bar[BAR_RED0 + r], 4);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -416,48 +545,97 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int ch = q4 * 32 + lane;             // channel = TMEM lane
         const bool ch_ok = ch < n;
         const uint32_t lane_addr = (uint32_t)(q4 * 32) << 16;
-        float ps[MM], po[MM], pc[MM], pr[MM];
+        // log2|y| of phase 1 is kept in tensor memory for phase 2 when it fits
+        constexpr bool kCacheL2 = kWG * MM <= kL2Chunks;
+        // mixtures (0,1), (2,3) as float2 pairs, an odd last one as a scalar
+        constexpr int NPR = MM / 2;
+        constexpr bool kOdd = (MM & 1) != 0;
+        constexpr int NPRA = NPR > 0 ? NPR : 1;
+        float pr[MM];
+        MixV<float2> P2[NPRA];
+        MixV<float> P1;
 #pragma unroll
         for (int j = 0; j < MM; j++) {
             const MixParam q = a.mp[((size_t)h * MM + j) * NP + (ch < NP ? ch : 0)];
-            ps[j] = ch < NP ? q.s : 0.f; po[j] = ch < NP ? q.off : 0.f;
-            pc[j] = ch < NP ? q.cl2 : 0.f; pr[j] = ch < NP ? q.rho : 1.f;
+            const float sj = ch < NP ? q.s : 0.f, oj = ch < NP ? -q.off : 0.f;
+            const float cj = ch < NP ? q.cl2 : 0.f, rj = ch < NP ? q.rho : 1.f;
+            pr[j] = rj;
+            if (j < 2 * NPR) {
+                float2* f[5] = {&P2[j / 2].s, &P2[j / 2].npo, &P2[j / 2].pc, &P2[j / 2].pr, &P2[j / 2].sr};
+                const float vals[5] = {sj, oj, cj, rj, sj * rj};
+#pragma unroll
+                for (int e = 0; e < 5; e++) {
+                    if (j & 1) f[e]->y = vals[e];
+                    else f[e]->x = vals[e];
+                }
+            } else {
+                P1.s = sj; P1.npo = oj; P1.pc = cj; P1.pr = rj; P1.sr = sj * rj;
+            }
         }
         const float wci = ch < NP ? a.wc[(size_t)h * NP + ch] : 0.f;
-        const float ltc_h = (float)(a.ltc64[h] - a.ltc64[0]);
         float ltc_all[kMaxModels];
 #pragma unroll
         for (int q = 0; q < kMaxModels; q++) ltc_all[q] = (q < M) ? (float)(a.ltc64[q] - a.ltc64[0]) : 0.f;
-        (void)ltc_all;
+        float* lse_sm = (float*)(sm + Sh::OFF_LSE) + (size_t)wg * kSub * 128 + ch;
 
-        float fUs[MM], fKn[MM], fLn[MM], fMn[MM], fMd[MM], fBd[MM], fRn[MM];
+        // Per (channel, mixture), with u = v z, p = |y|^rho, r = 1/y:
+        //   A0 = sum u, A1 = sum u p, A2 = sum u p^2, A3 = sum u p log2|y|,
+        //   A4 = sum u p r, A5 = sum u p r^2, A6 = sum u p^2 r^2.
+        // Since f' = rho sign(y)|y|^(rho-1) = rho p r, the reference's sums
+        // (src/kernels.cu:495-827) are: usum = A0, sum u f'^2 = rho^2 A6,
+        // sum u (f' y - 1)^2 = rho^2 A2 - 2 rho A1 + A0, sum u f' = rho A4,
+        // sum u f'/y = rho A5, sum u f' y = rho A1, sum u |y|^rho = A1,
+        // sum u |y|^rho log|y|^rho = rho ln2 A3.  They are formed in FP64 at
+        // each flush.
+        float2 fP[NPRA][7];
+        float fS1[7];
         float fCn = 0.f, fS2 = 0.f, fGs = 0.f;
+        auto zero_acc = [&]() {
 #pragma unroll
-        for (int j = 0; j < MM; j++) fUs[j] = fKn[j] = fLn[j] = fMn[j] = fMd[j] = fBd[j] = fRn[j] = 0.f;
+            for (int k = 0; k < 7; k++) {
+#pragma unroll
+                for (int q = 0; q < NPRA; q++) fP[q][k] = make_float2(0.f, 0.f);
+                fS1[k] = 0.f;
+            }
+            fCn = fS2 = fGs = 0.f;
+        };
+        auto acc_get = [&](int k, int j) -> float {
+            if (j < 2 * NPR) return (j & 1) ? fP[j / 2][k].y : fP[j / 2][k].x;
+            return fS1[k];
+        };
+        zero_acc();
         double dLL = 0.0, dVs = 0.0;
         // this thread's partial slot (one per warpgroup)
         PartLayout L{n, MM};
         double* out = a.partial + ((size_t)(cid * ta.ngroups + wg) * M + h) * L.stride();
-        double* out0 = a.partial + ((size_t)(cid * ta.ngroups) * M + h) * L.stride();  // Psi lives here
+        double* out0 = a.partial + ((size_t)(cid * ta.ngroups) * M + h) * L.stride();  // phi lives here
         auto flush = [&]() {
             if (ch_ok) {
 #pragma unroll
                 for (int j = 0; j < MM; j++) {
-                    out[L.mix(kUs) + j * n + ch] += fUs[j];
-                    out[L.mix(kKn) + j * n + ch] += fKn[j];
-                    out[L.mix(kLn) + j * n + ch] += fLn[j];
-                    out[L.mix(kMn) + j * n + ch] += fMn[j];
-                    out[L.mix(kMd) + j * n + ch] += fMd[j];
-                    out[L.mix(kBd) + j * n + ch] += fBd[j];
-                    out[L.mix(kRn) + j * n + ch] += fRn[j];
+                    const double r = (double)pr[j];
+                    const double A0 = acc_get(0, j), A1 = acc_get(1, j), A2 = acc_get(2, j);
+                    const double A3 = acc_get(3, j), A4 = acc_get(4, j), A5 = acc_get(5, j);
+                    const double A6 = acc_get(6, j);
+                    const int o = j * n + ch;
+                    red_add_f64(out + L.mix(kUs) + o, A0);
+                    red_add_f64(out + L.mix(kKn) + o, r * r * A6);
+                    red_add_f64(out + L.mix(kLn) + o, (r * r * A2 - 2.0 * r * A1) + A0);
+                    red_add_f64(out + L.mix(kMn) + o, r * A4);
+                    if (pr[j] <= 2.f || a.grad_mode) {
+                        red_add_f64(out + L.mix(kMd) + o, r * A5);
+                        red_add_f64(out + L.mix(kBd) + o, r * A1);
+                    } else {
+                        red_add_f64(out + L.mix(kMd) + o, r * r * A6);
+                        red_add_f64(out + L.mix(kBd) + o, A1);
+                    }
+                    if (a.update_rho) red_add_f64(out + L.mix(kRn) + o, r * kLn2 * A3);
                 }
-                out[L.cn() + ch] += fCn;
-                out[L.s2() + ch] += fS2;
-                out[L.gs() + ch] += fGs;
+                red_add_f64(out + L.cn() + ch, (double)fCn);
+                red_add_f64(out + L.s2() + ch, (double)fS2);
+                red_add_f64(out + L.gs() + ch, (double)fGs);
             }
-#pragma unroll
-            for (int j = 0; j < MM; j++) fUs[j] = fKn[j] = fLn[j] = fMn[j] = fMd[j] = fBd[j] = fRn[j] = 0.f;
-            fCn = fS2 = fGs = 0.f;
+            zero_acc();
         };
         // zero this thread's fields of the slot
         if (ch_ok) {
@@ -471,6 +649,14 @@ __global__ void __launch_bounds__(kThreads, 1)
             const int s = k & 1;
             const uint32_t u = (uint32_t)(k >> 1);
             const int64_t t0 = ((int64_t)cid + (int64_t)k * a.nclusters) * kS + wg * kSub;
+            // this tile's keep flags, fetched now and used after the exchange
+            const int64_t tk = t0 + (lane < kSub ? lane : kSub - 1);
+            const bool in_range = tk < a.T;
+            const bool kept = in_range && (a.keep == nullptr || a.keep[tk]);
+            const int par = k & 1;
+            uint64_t* ltbar = &bar[BAR_LT0 + par * kWG + wg];
+            // this tile's exchange: 4 warps x kSub samples x M models of 4 bytes
+            if (q4 == 0 && lane == 0) mbar_expect_tx(ltbar, (uint32_t)(4 * kSub * M * 4));
             ok = mbar_wait(&bar[BAR_BFULL0 + s], u & 1, abort_flag, a.err);
             if (!ok) break;
             tc_fence_after();
@@ -479,25 +665,39 @@ __global__ void __launch_bounds__(kThreads, 1)
             // ---- phase 1: per-sample log-sum-exp over mixtures (log2 units), 4 samples at a
             // time; the channel sum per sample is a 4-value transposed butterfly over the
             // warp's 32 lanes, after which lane 8q holds the warp's sum for sample 4g+q
+            uint32_t bnext[4];
+            tmem_ld4_nowait(bcol, bnext);
 #pragma unroll 1
             for (int g4 = 0; g4 < kSub / 4; g4++) {
-                float bx[4], v[4];
-                tmem_ld4(bcol + (uint32_t)(g4 * 4), bx);
+                float bx[4], v[4], l2c[MM][4];
+                tmem_wait_ld(bnext);
+#pragma unroll
+                for (int r = 0; r < 4; r++) bx[r] = __uint_as_float(bnext[r]);
+                if (g4 + 1 < kSub / 4) tmem_ld4_nowait(bcol + (uint32_t)(g4 * 4 + 4), bnext);
 #pragma unroll
                 for (int r = 0; r < 4; r++) {
-                    float q[MM], qmax = -INFINITY;
+                    float q[MM];
 #pragma unroll
-                    for (int j = 0; j < MM; j++) {
-                        const float y = fmaf(ps[j], bx[r], -po[j]);
-                        const float ay = fmaxf(fabsf(y), kTinyAbs);
-                        const float p = ptx_ex2(pr[j] * ptx_lg2(ay));
-                        q[j] = fmaf(-p, kLog2e, pc[j]);
-                        qmax = fmaxf(qmax, q[j]);
+                    for (int qq = 0; qq < NPR; qq++) {
+                        float2 L2;
+                        const float2 q2 = dens_q(P2[qq], bx[r], L2);
+                        q[2 * qq] = q2.x; q[2 * qq + 1] = q2.y;
+                        l2c[2 * qq][r] = L2.x; l2c[2 * qq + 1][r] = L2.y;
                     }
-                    float se = 0.f;
+                    if constexpr (kOdd) {
+                        float L2;
+                        q[MM - 1] = dens_q(P1, bx[r], L2);
+                        l2c[MM - 1][r] = L2;
+                    }
+                    const float lse = lse2<MM>(q);
+                    lse_sm[(g4 * 4 + r) * 128] = lse;
+                    v[r] = ch_ok ? lse : 0.f;
+                }
+                if constexpr (kCacheL2) {
 #pragma unroll
-                    for (int j = 0; j < MM; j++) se += ptx_ex2(q[j] - qmax);
-                    v[r] = ch_ok ? qmax + ptx_lg2(se) : 0.f;
+                    for (int j = 0; j < MM; j++)
+                        tmem_st4_nowait(tmem + lane_addr + l2_chunk_col(wg * MM + j) + (uint32_t)(g4 * 4),
+                                        l2c[j]);
                 }
                 {
                     const bool up16 = (lane & 16) != 0;
@@ -511,43 +711,30 @@ __global__ void __launch_bounds__(kThreads, 1)
                     w += __shfl_xor_sync(0xffffffffu, w, 4);
                     w += __shfl_xor_sync(0xffffffffu, w, 2);
                     w += __shfl_xor_sync(0xffffffffu, w, 1);
-                    // lane bits (4,3) select the sample: 2*bit4 + bit3
-                    if ((lane & 7) == 0)
-                        red[(((k & 1) * kWG + wg) * 4 + q4) * 16 + g4 * 4 + ((lane >> 4) & 1) * 2 +
-                            ((lane >> 3) & 1)] = w;
+                    // lane bits (4,3) select the sample: 2*bit4 + bit3; the warp's sum
+                    // goes to every model's CTA
+                    if ((lane & 7) == 0) {
+                        const int t = wg * kSub + g4 * 4 + ((lane >> 4) & 1) * 2 + ((lane >> 3) & 1);
+                        const uint32_t sl = smem_u32(slot + ((par * kMaxModels + h) * 4 + q4) * kS + t);
+                        const uint32_t lb = smem_u32(ltbar);
+                        for (int q = 0; q < M; q++) st_async_f32(mapa(sl, (uint32_t)q), w, mapa(lb, (uint32_t)q));
+                    }
                 }
             }
-            // the four warps of this warpgroup combine; lanes 0-15 of warp q4 == 0 publish
-            const int par = k & 1;
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&bar[BAR_RED0 + par * kWG + wg]);
-            if (q4 == 0) {
-                ok = mbar_wait(&bar[BAR_RED0 + par * kWG + wg], u & 1, abort_flag, a.err);
-                if (!ok) break;
-            }
-            if (q4 == 0 && lane < 16) {
-                const float* rr = red + ((par * kWG + wg) * 4) * 16;
-                const float s4 = rr[0 * 16 + lane] + rr[1 * 16 + lane] + rr[2 * 16 + lane] + rr[3 * 16 + lane];
-                const float Lh = ltc_h + kLn2 * s4;
-                const uint32_t sl = smem_u32(slot + (par * kMaxModels + h) * kS + wg * kSub + lane);
-                const uint32_t lb = smem_u32(&bar[BAR_LT0 + par]);
-                for (int q = 0; q < M; q++) {
-                    st_cluster_f32(mapa(sl, (uint32_t)q), Lh);
-                    mbar_arrive_remote(mapa(lb, (uint32_t)q));
-                }
-            }
-            ok = mbar_wait(&bar[BAR_LT0 + par], u & 1, abort_flag, a.err, true);
+            if constexpr (kCacheL2) tmem_wait_st();
+            ok = mbar_wait(ltbar, u & 1, abort_flag, a.err, true);
             if (!ok) break;
-            // ---- P(t), v_h(t): lanes 0-15 of every warp, one sample each
+            // ---- P(t), v_h(t): lanes < kSub of every warp, one sample each
             float vme = 0.f;
             {
-                const int t = lane & 15;
+                const int t = lane < kSub ? lane : kSub - 1;
                 float Lq[kMaxModels];
                 float lmax = -INFINITY;
 #pragma unroll
                 for (int q = 0; q < kMaxModels; q++) {
                     if (q < M) {
-                        Lq[q] = slot[(par * kMaxModels + q) * kS + wg * kSub + t];
+                        const float* sq = slot + (par * kMaxModels + q) * 4 * kS + wg * kSub + t;
+                        Lq[q] = ltc_all[q] + kLn2 * (((sq[0] + sq[kS]) + sq[2 * kS]) + sq[3 * kS]);
                         lmax = fmaxf(lmax, Lq[q]);
                     }
                 }
@@ -561,15 +748,15 @@ __global__ void __launch_bounds__(kThreads, 1)
                 for (int q = 0; q < kMaxModels; q++)
                     if (q == h) Lmine = Lq[q];
                 const float vh = ptx_ex2((Lmine - P) * kLog2e);
-                const int64_t tg = t0 + t;
-                const bool valid = tg < a.T && (a.keep == nullptr || a.keep[tg]);
+                const int64_t tg = tk;
+                const bool valid = kept;
                 vme = valid ? vh : 0.f;
-                if (q4 == 0 && lane < 16) {
+                if (q4 == 0 && lane < kSub) {
                     if (valid) {
                         dVs += (double)vh;
                         if (h == 0) dLL += (double)P;
                     }
-                    if (tg < a.T) {
+                    if (in_range) {
                         if (a.Lt_out) a.Lt_out[(size_t)h * a.T + tg] = Lmine;
                         if (a.P_out && h == 0) a.P_out[tg] = P;
                     }
@@ -583,48 +770,43 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll 1
             for (int g4 = 0; g4 < kSub / 4; g4++) {
                 float bx[4], gq[4], bq[4];
-                tmem_ld4(bcol + (uint32_t)(g4 * 4), bx);
+                uint32_t l2r[MM][4];
+                {
+                    uint32_t br[4];
+                    tmem_ld4_nowait(bcol + (uint32_t)(g4 * 4), br);
+                    if constexpr (kCacheL2) {
+#pragma unroll
+                        for (int j = 0; j < MM; j++)
+                            tmem_ld4_nowait(tmem + lane_addr + l2_chunk_col(wg * MM + j) + (uint32_t)(g4 * 4),
+                                            l2r[j]);
+                    }
+                    tmem_wait_ld(br);
+                    if constexpr (kCacheL2) {
+#pragma unroll
+                        for (int j = 0; j < MM; j++) tmem_wait_ld(l2r[j]);
+                    }
+#pragma unroll
+                    for (int r = 0; r < 4; r++) bx[r] = __uint_as_float(br[r]);
+                }
 #pragma unroll
                 for (int r = 0; r < 4; r++) {
                     const float v = __shfl_sync(0xffffffffu, vme, g4 * 4 + r);
-                    float y[MM], L2[MM], p[MM], q[MM], qmax = -INFINITY;
+                    const float lse = lse_sm[(g4 * 4 + r) * 128];
+                    float2 g2 = make_float2(0.f, 0.f);
+                    float g1 = 0.f;
 #pragma unroll
-                    for (int j = 0; j < MM; j++) {
-                        y[j] = fmaf(ps[j], bx[r], -po[j]);
-                        const float ay = fmaxf(fabsf(y[j]), kTinyAbs);
-                        L2[j] = ptx_lg2(ay);
-                        p[j] = ptx_ex2(pr[j] * L2[j]);
-                        q[j] = fmaf(-p[j], kLog2e, pc[j]);
-                        qmax = fmaxf(qmax, q[j]);
+                    for (int qq = 0; qq < NPR; qq++) {
+                        float2 L2 = make_float2(0.f, 0.f);
+                        if constexpr (kCacheL2)
+                            L2 = make_float2(__uint_as_float(l2r[2 * qq][r]), __uint_as_float(l2r[2 * qq + 1][r]));
+                        dens_acc<float2, kCacheL2>(P2[qq], bx[r], L2, -lse, v, fP[qq], g2);
                     }
-                    float e[MM], se = 0.f;
-#pragma unroll
-                    for (int j = 0; j < MM; j++) { e[j] = ptx_ex2(q[j] - qmax); se += e[j]; }
-                    const float vr = v * ptx_rcp(se);
-                    float g = 0.f;
-#pragma unroll
-                    for (int j = 0; j < MM; j++) {
-                        const float uu = e[j] * vr;
-                        const float ay = fmaxf(fabsf(y[j]), kTinyAbs);
-                        const float ri = ptx_rcp(ay);
-                        const float pm1 = p[j] * ri;
-                        const float fp = copysignf(pr[j] * pm1, y[j]);
-                        const float ufp = uu * fp;
-                        g = fmaf(ps[j], ufp, g);
-                        fUs[j] += uu;
-                        fKn[j] = fmaf(ufp, fp, fKn[j]);
-                        const float lv = fmaf(fp, y[j], -1.f);
-                        fLn[j] = fmaf(uu * lv, lv, fLn[j]);
-                        fMn[j] += ufp;
-                        if (pr[j] <= 2.f || a.grad_mode) {
-                            fMd[j] = fmaf(ufp, copysignf(ri, y[j]), fMd[j]);
-                            fBd[j] = fmaf(ufp, y[j], fBd[j]);
-                        } else {
-                            fMd[j] = fmaf(ufp, fp, fMd[j]);
-                            fBd[j] = fmaf(uu, p[j], fBd[j]);
-                        }
-                        if (a.update_rho) fRn[j] = fmaf(uu * p[j], pr[j] * L2[j] * kLn2, fRn[j]);
+                    if constexpr (kOdd) {
+                        float L2 = 0.f;
+                        if constexpr (kCacheL2) L2 = __uint_as_float(l2r[MM - 1][r]);
+                        dens_acc<float, kCacheL2>(P1, bx[r], L2, -lse, v, fS1, g1);
                     }
+                    float g = (g2.x + g2.y) + g1;
                     const float bb = bx[r] - wci;
                     fCn = fmaf(v, bb, fCn);
                     fS2 = fmaf(v * bb, bb, fS2);

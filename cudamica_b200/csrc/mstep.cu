@@ -34,246 +34,176 @@ __device__ double block_sum(double v, double* sh) {
 }
 
 // ---------------------------------------------------------------------------
-// k_prep: W_h = A_h^{-1} (Gauss-Jordan, partial pivoting), ldet_h = -log|det A_h|
-// and the FP32 constants of the E-step.  One CTA per model.
-// Replaces pinv() + the ldet computation (src/amica.cu:27-127, :835-924).
-__global__ void __launch_bounds__(kT) k_prep(
+// k_inverse_derive: W_h = A_h^{-1}, ldet_h = -log|det A_h| and the FP32 E-step
+// constants, one CTA of 512 threads per model (n <= 128).  Replaces pinv() and
+// the LU log-determinant (src/amica.cu:27-127, :864-924).
+//
+// Gauss-Jordan elimination with partial pivoting and no row interchanges: the
+// pivot of column k is the not yet used row p_k with the largest |a(p_k, k)|
+// (lowest row on ties).  Eliminating in place turns column k of the working
+// matrix into column p_k of P.A^{-1}, so at the end W(j, p_k) = a(p_j, k).
+// Thread (g, c) = (tid / 128, tid % 128) keeps a(g + 4 i, c), i < 32, in
+// registers.  A pivot step costs two barriers: the owners of column k publish it
+// with their argmax candidates, then the pivot row is published.  Row p is
+// reached in the register array through a switch on the (uniform) index p / 4.
+constexpr int kInvThreads = 512;
+constexpr int kInvGroups = kInvThreads / 128;         // row groups
+constexpr int kInvRows = 128 / kInvGroups;            // rows per thread (32)
+
+#define AMICA_CASES32(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) \
+    X(13) X(14) X(15) X(16) X(17) X(18) X(19) X(20) X(21) X(22) X(23) X(24) X(25) X(26) X(27)   \
+    X(28) X(29) X(30) X(31)
+
+__device__ __forceinline__ double reg_get(const double (&a)[kInvRows], int i) {
+    double v = 0.0;
+#define AMICA_GET(k) case k: v = a[k]; break;
+    switch (i) { AMICA_CASES32(AMICA_GET) default: break; }
+#undef AMICA_GET
+    return v;
+}
+__device__ __forceinline__ void reg_set(double (&a)[kInvRows], int i, double v) {
+#define AMICA_SET(k) case k: a[k] = v; break;
+    switch (i) { AMICA_CASES32(AMICA_SET) default: break; }
+#undef AMICA_SET
+}
+
+__global__ void __launch_bounds__(kInvThreads, 1) k_inverse_derive(
     const double* __restrict__ A, const double* __restrict__ c, const double* __restrict__ alpha,
     const double* __restrict__ mu, const double* __restrict__ beta, const double* __restrict__ rho,
-    const double* __restrict__ gm, double ldetS, double* __restrict__ aug, double* __restrict__ W,
-    double* __restrict__ ldet, double* __restrict__ ltc64, float* __restrict__ Wf,
-    float* __restrict__ wcf, MixParam* __restrict__ mp, int n, int m, int NP, int* err) {
+    const double* __restrict__ gm, double ldetS, double* __restrict__ W, double* __restrict__ ldet,
+    double* __restrict__ ltc64, float* __restrict__ Wf, float* __restrict__ wcf,
+    MixParam* __restrict__ mp, int n, int m, int NP, int* err) {
+    extern __shared__ double Ws[];                    // [n][n] row-major W_h, after elimination
+    // colk[buf][g * 32 + i] = a(g + 4 i, k): each thread's rows are contiguous
+    __shared__ __align__(16) double colk[2][128];
+    __shared__ double prow[2][128], cval[2][kInvGroups], pivs[128], wcs[128];
+    __shared__ int cidx[2][kInvGroups], perm[128], pinv[128];
     const int h = blockIdx.x, tid = threadIdx.x;
-    const int n2 = 2 * n;
-    double* a = aug + (size_t)h * n * n2;              // row-major [r][c], c < 2n
-    const double* Ah = A + (size_t)h * n * n;          // column-major
-    __shared__ double fcol[256];
-    __shared__ double sh[33];
-    __shared__ int piv_s;
-    __shared__ double pv_s;
-    for (int e = tid; e < n * n2; e += kT) {
-        const int r = e / n2, cc = e % n2;
-        a[e] = (cc < n) ? Ah[(size_t)cc * n + r] : ((cc - n) == r ? 1.0 : 0.0);
-    }
-    __syncthreads();
-    double logdet = 0.0;
-    bool singular = false;
-    for (int k = 0; k < n; k++) {
-        // pivot: argmax_{r >= k} |a(r,k)| (lowest index on ties)
-        double best = -1.0;
-        int bi = k;
-        for (int r = k + tid; r < n; r += kT) {
-            const double v = fabs(a[(size_t)r * n2 + k]);
-            if (v > best) { best = v; bi = r; }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-        }
-        __shared__ double wb[8];
-        __shared__ int wi[8];
-        if (tid % 32 == 0) { wb[tid / 32] = best; wi[tid / 32] = bi; }
-        __syncthreads();
-        if (tid == 0) {
-            double b = wb[0];
-            int i = wi[0];
-            for (int w = 1; w < kT / 32; w++)
-                if (wb[w] > b || (wb[w] == b && wi[w] < i)) { b = wb[w]; i = wi[w]; }
-            piv_s = i;
-        }
-        __syncthreads();
-        const int p = piv_s;
-        if (p != k)
-            for (int cc = tid; cc < n2; cc += kT) {
-                const double t = a[(size_t)k * n2 + cc];
-                a[(size_t)k * n2 + cc] = a[(size_t)p * n2 + cc];
-                a[(size_t)p * n2 + cc] = t;
-            }
-        __syncthreads();
-        if (tid == 0) pv_s = a[(size_t)k * n2 + k];
-        __syncthreads();
-        const double pv = pv_s;
-        if (pv == 0.0) { singular = true; break; }
-        logdet += log(fabs(pv));
-        const double inv = 1.0 / pv;
-        for (int cc = tid; cc < n2; cc += kT) a[(size_t)k * n2 + cc] *= inv;
-        for (int r = tid; r < n; r += kT) fcol[r] = a[(size_t)r * n2 + k];
-        __syncthreads();
-        for (int e = tid; e < n * n2; e += kT) {
-            const int r = e / n2, cc = e % n2;
-            if (r != k) a[e] -= fcol[r] * a[(size_t)k * n2 + cc];
-        }
-        __syncthreads();
-    }
-    if (singular) {
-        if (tid == 0) atomicOr(err, kErrSingular);
-        return;
-    }
-    double* Wh = W + (size_t)h * n * n;
-    for (int e = tid; e < n * n; e += kT) {
-        const int r = e % n, cc = e / n;
-        Wh[e] = a[(size_t)r * n2 + n + cc];             // column-major W(r, cc)
-    }
-    if (tid == 0) {
-        ldet[h] = -logdet;
-        ltc64[h] = log(gm[h]) - logdet + ldetS;         // src/amica.cu:1009
-    }
-    __syncthreads();
-    // FP32 copies for the E-step
-    float* Wfh = Wf + (size_t)h * NP * NP;
-    for (int e = tid; e < NP * NP; e += kT) {
-        const int i = e / NP, k = e % NP;
-        Wfh[e] = (i < n && k < n) ? (float)Wh[(size_t)k * n + i] : 0.f;
-    }
-    for (int i = tid; i < NP; i += kT) {
-        double wc = 0.0;
-        if (i < n)
-            for (int k = 0; k < n; k++) wc += Wh[(size_t)k * n + i] * c[(size_t)h * n + k];
-        wcf[(size_t)h * NP + i] = (float)wc;
-        for (int j = 0; j < m; j++) {
-            MixParam q;
-            if (i < n) {
-                const size_t idx = ((size_t)h * m + j) * n + i;
-                const double s = sqrt(beta[idx]);
-                const double r = rho[idx];
-                q.s = (float)s;
-                q.off = (float)(s * (mu[idx] + wc));
-                q.cl2 = (float)((log(alpha[idx]) + 0.5 * log(beta[idx]) - M_LN2 - lgamma(1.0 + 1.0 / r)) *
-                                1.4426950408889634);
-                q.rho = (float)r;
-            } else {
-                q.s = 0.f; q.off = 0.f; q.cl2 = 0.f; q.rho = 1.f;
-            }
-            mp[((size_t)h * m + j) * NP + i] = q;
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// k_inverse_smem: W_h = A_h^{-1} by in-place Gauss-Jordan with partial pivoting,
-// the whole n x n FP64 matrix resident in shared memory (n <= 128), one CTA of
-// 1024 threads per model; ldet_h = -sum log|pivot|.  Replaces pinv() and the
-// LU log-determinant (src/amica.cu:27-127, :864-924).
-__global__ void __launch_bounds__(1024) k_inverse_smem(const double* __restrict__ A,
-                                                       const double* __restrict__ gm, double ldetS,
-                                                       double* __restrict__ W,
-                                                       double* __restrict__ ldet,
-                                                       double* __restrict__ ltc64, int n, int* err) {
-    extern __shared__ double gj[];                       // [n][n] row-major, then fcol[n]
-    double* fcol = gj + n * n;
-    __shared__ int perm[128];
-    __shared__ double wb[32];
-    __shared__ int wi[32];
-    __shared__ double piv_s, logdet_s;
-    __shared__ int p_s, bad_s;
-    const int h = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+    const int g = tid >> 7, col = tid & 127;
     const double* Ah = A + (size_t)h * n * n;
-    for (int e = tid; e < n * n; e += nt) {
-        const int r = e / n, c = e % n;
-        gj[e] = Ah[(size_t)c * n + r];
+    double a[kInvRows];
+#pragma unroll
+    for (int i = 0; i < kInvRows; i++) {
+        const int r = g + kInvGroups * i;
+        a[i] = (r < n && col < n) ? Ah[(size_t)col * n + r] : 0.0;
     }
-    if (tid == 0) { logdet_s = 0.0; bad_s = 0; }
-    __syncthreads();
+    unsigned used = 0;                                // bit i: row g + 4 i is a pivot row
+    bool bad = false;
+    // Publishing pivot column oc: in each group, the warp that holds column oc
+    // stores it (its owner lane), then picks the group's candidate with a warp
+    // argmax over 32-bit keys: |a| rounded down to 18 mantissa bits above the
+    // row slot, lowest row on ties (the groups' candidates are then compared
+    // exactly).  The candidate's reciprocal is formed here, off the pivot path.
+    __shared__ double cinv[2][kInvGroups];
+    const int warp = tid >> 5, lane = tid & 31;
+    auto publish = [&](int oc, int buf) {
+        if ((warp & 3) != (oc >> 5)) return;          // warp-uniform
+        if (col == oc) {
+#pragma unroll
+            for (int i = 0; i < kInvRows; i += 2)
+                *reinterpret_cast<double2*>(&colk[buf][g * kInvRows + i]) = make_double2(a[i], a[i + 1]);
+        }
+        __syncwarp();
+        const double v = colk[buf][g * kInvRows + lane];
+        const bool usable = (g + kInvGroups * lane < n) && !((used >> lane) & 1u);
+        uint32_t key = usable ? ((__float_as_uint((float)fabs(v)) & ~31u) | (uint32_t)(31 - lane)) + 32u : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) key = max(key, __shfl_xor_sync(0xffffffffu, key, o));
+        if (lane == 0) {
+            const int ib = 31 - (int)(key & 31u);
+            const double pv = colk[buf][g * kInvRows + ib];
+            cval[buf][g] = key ? fabs(pv) : -1.0;
+            cidx[buf][g] = key ? g + kInvGroups * ib : 0x7fffffff;
+            cinv[buf][g] = key ? 1.0 / pv : 0.0;
+        }
+    };
+    publish(0, 0);
     for (int k = 0; k < n; k++) {
-        // pivot row: argmax_{r >= k} |a(r,k)|, lowest index on ties
-        double best = -1.0;
-        int bi = k;
-        for (int r = k + tid; r < n; r += nt) {
-            const double v = fabs(gj[r * n + k]);
-            if (v > best) { best = v; bi = r; }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-        }
-        if ((tid & 31) == 0) { wb[tid >> 5] = best; wi[tid >> 5] = bi; }
+        const int buf = k & 1;
         __syncthreads();
-        if (tid == 0) {
-            double b = wb[0];
-            int i = wi[0];
-            for (int w = 1; w < nt / 32; w++)
-                if (wb[w] > b || (wb[w] == b && wi[w] < i)) { b = wb[w]; i = wi[w]; }
-            p_s = i;
-            perm[k] = i;
+        double best = cval[buf][0];
+        int p = cidx[buf][0];
+        int gb = 0;
+#pragma unroll
+        for (int q = 1; q < kInvGroups; q++) {
+            const double v = cval[buf][q];
+            const int r = cidx[buf][q];
+            if (v > best || (v == best && r < p)) { best = v; p = r; gb = q; }
         }
+        if (!(best > 0.0)) { bad = true; break; }    // same decision in every thread
+        const int gp = p % kInvGroups, ip = p / kInvGroups;
+        const double inv = cinv[buf][gb];
+        if (g == gp) {
+            prow[buf][col] = reg_get(a, ip);
+            used |= 1u << ip;
+        }
+        if (tid == 0) { perm[k] = p; pinv[p] = k; pivs[k] = colk[buf][gp * kInvRows + ip]; }
         __syncthreads();
-        const int p = p_s;
-        if (p != k)
-            for (int c = tid; c < n; c += nt) {
-                const double t = gj[k * n + c];
-                gj[k * n + c] = gj[p * n + c];
-                gj[p * n + c] = t;
+        const double pc = prow[buf][col] * inv;       // a(p, col) / piv
+        if (col == k) {
+#pragma unroll
+            for (int i = 0; i < kInvRows; i++) a[i] = -a[i] * inv;
+        } else {
+            const double* f = &colk[buf][g * kInvRows];
+#pragma unroll
+            for (int i = 0; i < kInvRows; i += 2) {
+                const double2 f2 = *reinterpret_cast<const double2*>(f + i);
+                a[i] = fma(-f2.x, pc, a[i]);
+                a[i + 1] = fma(-f2.y, pc, a[i + 1]);
             }
-        __syncthreads();
-        if (tid == 0) {
-            piv_s = gj[k * n + k];
-            if (piv_s == 0.0) bad_s = 1;
-            else logdet_s += log(fabs(piv_s));
         }
-        for (int r = tid; r < n; r += nt) fcol[r] = gj[r * n + k];
-        __syncthreads();
-        if (bad_s) break;
-        const double inv = 1.0 / piv_s;
-        for (int c = tid; c < n; c += nt) gj[k * n + c] = (c == k ? 1.0 : gj[k * n + c]) * inv;
-        __syncthreads();
-        for (int e = tid; e < n * n; e += nt) {
-            const int r = e / n, c = e % n;
-            if (r != k) gj[e] = (c == k ? 0.0 : gj[e]) - fcol[r] * gj[k * n + c];
-        }
-        __syncthreads();
+        if (g == gp) reg_set(a, ip, col == k ? inv : pc);
+        if (k + 1 < n) publish(k + 1, buf ^ 1);
     }
-    if (bad_s) {
+    if (bad) {
         if (tid == 0) atomicOr(err, kErrSingular);
         return;
     }
-    // undo the row interchanges as column interchanges, last first
-    for (int k = n - 1; k >= 0; k--) {
-        const int p = perm[k];
-        if (p != k)
-            for (int r = tid; r < n; r += nt) {
-                const double t = gj[r * n + k];
-                gj[r * n + k] = gj[r * n + p];
-                gj[r * n + p] = t;
-            }
-        __syncthreads();
-    }
+    __syncthreads();
+    // W(j, p_k) = a(p_j, k): row-major copy in shared memory and column-major W_h
     double* Wh = W + (size_t)h * n * n;
-    for (int e = tid; e < n * n; e += nt) {
-        const int r = e % n, c = e / n;
-        Wh[e] = gj[r * n + c];                          // column-major W(r, c)
+#pragma unroll
+    for (int i = 0; i < kInvRows; i++) {
+        const int r = g + kInvGroups * i;
+        if (r < n && col < n) {
+            const int j = pinv[r], kk = perm[col];
+            Ws[j * n + kk] = a[i];
+            Wh[(size_t)kk * n + j] = a[i];
+        }
     }
+    if (tid < n) pivs[tid] = log(fabs(pivs[tid]));
+    __syncthreads();
     if (tid == 0) {
-        ldet[h] = -logdet_s;
-        ltc64[h] = log(gm[h]) - logdet_s + ldetS;       // src/amica.cu:1009
+        double ld = 0.0;
+        for (int k = 0; k < n; k++) ld += pivs[k];
+        ldet[h] = -ld;
+        ltc64[h] = log(gm[h]) - ld + ldetS;           // src/amica.cu:1009
     }
-}
-
-// FP32 E-step constants from W and the parameters (grid: models x channel blocks).
-__global__ void __launch_bounds__(128) k_derive(
-    const double* __restrict__ W, const double* __restrict__ c, const double* __restrict__ alpha,
-    const double* __restrict__ mu, const double* __restrict__ beta, const double* __restrict__ rho,
-    float* __restrict__ Wf, float* __restrict__ wcf, MixParam* __restrict__ mp, int n, int m,
-    int NP) {
-    const int h = blockIdx.x;
-    const int i = blockIdx.y * blockDim.x + threadIdx.x;   // channel
-    if (i >= NP) return;
-    const double* Wh = W + (size_t)h * n * n;
+    // E-step constants: W in FP32 (row-major, NP x NP, zero padded), w_c = W c,
+    // and per (mixture, channel) sqrt(beta), sqrt(beta)(mu + w_c), the log2
+    // normaliser and rho
+    if (tid < NP) {
+        double wc = 0.0;
+        if (tid < n)
+            for (int k = 0; k < n; k++) wc += Ws[tid * n + k] * c[(size_t)h * n + k];
+        wcs[tid] = wc;
+        wcf[(size_t)h * NP + tid] = (float)wc;
+    }
     float* Wfh = Wf + (size_t)h * NP * NP;
-    for (int k = 0; k < NP; k++) Wfh[(size_t)i * NP + k] = (i < n && k < n) ? (float)Wh[(size_t)k * n + i] : 0.f;
-    double wc = 0.0;
-    if (i < n)
-        for (int k = 0; k < n; k++) wc += Wh[(size_t)k * n + i] * c[(size_t)h * n + k];
-    wcf[(size_t)h * NP + i] = (float)wc;
-    for (int j = 0; j < m; j++) {
+    for (int e = tid; e < NP * NP; e += kInvThreads) {
+        const int i = e / NP, k = e - i * NP;
+        Wfh[e] = (i < n && k < n) ? (float)Ws[i * n + k] : 0.f;
+    }
+    __syncthreads();
+    for (int e = tid; e < m * NP; e += kInvThreads) {
+        const int j = e / NP, i = e - j * NP;
         MixParam q;
         if (i < n) {
             const size_t idx = ((size_t)h * m + j) * n + i;
             const double s = sqrt(beta[idx]);
             const double r = rho[idx];
             q.s = (float)s;
-            q.off = (float)(s * (mu[idx] + wc));
+            q.off = (float)(s * (mu[idx] + wcs[i]));
             q.cl2 = (float)((log(alpha[idx]) + 0.5 * log(beta[idx]) - M_LN2 - lgamma(1.0 + 1.0 / r)) *
                             1.4426950408889634);
             q.rho = (float)r;
@@ -284,25 +214,57 @@ __global__ void __launch_bounds__(128) k_derive(
     }
 }
 
+// Entry (r, cc) of the A-update matrix B_h (src/amica.cu:2155-2279,
+// src/kernels.cu:961-1014): the Newton form when this model takes the Newton
+// step, else the natural gradient I - phi / vsum.
+__device__ __forceinline__ double b_entry(const double* __restrict__ phi, double ivs,
+                                          const double* __restrict__ kappa,
+                                          const double* __restrict__ lambda,
+                                          const double* __restrict__ sig2, int newton, int r, int cc,
+                                          int n) {
+    const double prc = phi[(size_t)cc * n + r] * ivs;      // phi(r, c) / vsum
+    if (newton) {
+        if (r == cc) return (1.0 - prc) / lambda[r];
+        const double pcr = phi[(size_t)r * n + cc] * ivs;
+        const double nom = -sig2[r] * kappa[cc];
+        return (nom * (-prc) + (-pcr)) / ((kappa[r] * sig2[r]) * (kappa[cc] * sig2[cc]) - 1.0);
+    }
+    return (r == cc ? 1.0 : 0.0) - prc;
+}
+
 // Batched FP64 32x32-tiled products on n x n column-major matrices, one
 // (tile, model) per CTA of 256 threads:
-//   kind 0 (A update, src/amica.cu:2330-2342):  Out = X + s_h X Y,
-//          s_h = +lrate (Newton) or -lrate (natural gradient)
+//   kind 0 (A update, src/amica.cu:2330-2342):  Out = X + s_h X B_h,
+//          s_h = +lrate (Newton) or -lrate (natural gradient), B_h formed
+//          on the fly from phi, kappa, lambda and sigma2
 //   kind 1 (phi from Psi):  Out = (Psi - gsum c^T) W^T, written into the
 //          statistics vector's phi block
-__global__ void __launch_bounds__(256) k_gemm64(int kind, const double* __restrict__ X,
-                                                size_t strideX, const double* __restrict__ Y,
-                                                size_t strideY, double* __restrict__ Out,
-                                                size_t strideOut, const double* __restrict__ gs,
-                                                size_t strideG, const double* __restrict__ c,
-                                                const int* __restrict__ use_newton,
-                                                const Ctrl* __restrict__ ctrl, int n) {
+struct GemmArgs {
+    int kind, n, m;
+    const double* X; size_t strideX;
+    const double* Y; size_t strideY;        // kind 1: W
+    double* Out; size_t strideOut;
+    const double* gs; size_t strideG;       // kind 1
+    const double* c;                        // kind 1
+    const int* use_newton;                  // kind 0
+    const Ctrl* ctrl;                       // kind 0
+    const double* stats;                    // kind 0: phi and vsum
+    const double* work;                     // kind 0: kappa, lambda, sigma2
+};
+
+__global__ void __launch_bounds__(256) k_gemm64(GemmArgs g) {
     __shared__ double xs[32][33], ys[32][33];
+    const int n = g.n;
     const int h = blockIdx.z;
     const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
     const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;   // ty: 0..7
-    const double* Xh = X + strideX * h;
-    const double* Yh = Y + strideY * h;
+    const double* Xh = g.X + g.strideX * h;
+    const double* Yh = g.kind == 1 ? g.Y + g.strideY * h : nullptr;
+    StatLayout SL{n, g.m};
+    const double* phi = g.kind == 0 ? g.stats + SL.base(h) + SL.phi() : nullptr;
+    const double ivs = g.kind == 0 ? 1.0 / g.stats[SL.base(h) + SL.vs()] : 0.0;
+    const double* kappa = g.kind == 0 ? g.work + (size_t)h * 4 * n : nullptr;
+    const int newton = g.kind == 0 ? g.use_newton[h] : 0;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (int k0 = 0; k0 < n; k0 += 32) {
         for (int q = 0; q < 4; q++) {
@@ -312,13 +274,15 @@ __global__ void __launch_bounds__(256) k_gemm64(int kind, const double* __restri
             double xv = 0.0;
             if (r < n && k < n) {
                 xv = Xh[(size_t)k * n + r];
-                if (kind == 1) xv -= gs[strideG * h + r] * c[(size_t)h * n + k];
+                if (g.kind == 1) xv -= g.gs[g.strideG * h + r] * g.c[(size_t)h * n + k];
             }
             xs[tx][rr] = xv;
-            // Y(k0 + rr, c0 + tx): kind 0 -> Y col-major; kind 1 -> W^T(k, col) = W(col, k)
+            // Y(k0 + rr, c0 + tx): kind 0 -> B_h(k, col); kind 1 -> W^T(k, col) = W(col, k)
             const int col = c0 + tx;
             double yv = 0.0;
-            if (k < n && col < n) yv = (kind == 0) ? Yh[(size_t)col * n + k] : Yh[(size_t)k * n + col];
+            if (k < n && col < n)
+                yv = (g.kind == 0) ? b_entry(phi, ivs, kappa, kappa + n, kappa + 2 * n, newton, k, col, n)
+                                   : Yh[(size_t)k * n + col];
             ys[rr][tx] = yv;
         }
         __syncthreads();
@@ -333,51 +297,62 @@ __global__ void __launch_bounds__(256) k_gemm64(int kind, const double* __restri
     const int r = r0 + tx;
     if (r >= n) return;
     double s = 1.0;
-    if (kind == 0) s = use_newton[h] ? ctrl->lrate : -ctrl->lrate;
+    if (g.kind == 0) s = newton ? g.ctrl->lrate : -g.ctrl->lrate;
     for (int q = 0; q < 4; q++) {
         const int col = c0 + ty + 8 * q;
         if (col >= n) continue;
-        double* o = Out + strideOut * h + (size_t)col * n + r;
-        if (kind == 0) *o = Xh[(size_t)col * n + r] + s * acc[q];
+        double* o = g.Out + g.strideOut * h + (size_t)col * n + r;
+        if (g.kind == 0) *o = Xh[(size_t)col * n + r] + s * acc[q];
         else *o = acc[q];
     }
 }
 
 // Reparametrisation and c update after the A update (src/amica.cu:2367-2512):
 // unit columns of A, mu *= norm, beta /= norm^2, mu -= W_old (cnew - c), c = cnew.
-__global__ void __launch_bounds__(256) k_reparm(int update_A, int do_reparm, double* A,
-                                                const double* __restrict__ Anew,
-                                                const double* __restrict__ W, double* c,
-                                                double* mu, double* beta,
-                                                const double* __restrict__ work, int n, int m) {
-    const int h = blockIdx.x, tid = threadIdx.x;
+// One CTA of 1024 threads per model (n <= 128).
+__global__ void __launch_bounds__(1024) k_reparm(int update_A, int do_reparm, double* A,
+                                                 const double* __restrict__ Anew,
+                                                 const double* __restrict__ W, double* c,
+                                                 double* mu, double* beta,
+                                                 const double* __restrict__ work, int n, int m) {
+    const int h = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const double* cnew = work + (size_t)h * 4 * n + 3 * n;
     double* ch = c + (size_t)h * n;
-    __shared__ double norms[256];
-    __shared__ double shift[256];
+    __shared__ double norms[128], shift[128], dc[128];
     if (update_A) {
         double* Ah = A + (size_t)h * n * n;
         const double* An = Anew + (size_t)h * n * n;
         if (do_reparm) {
-            for (int cc = tid; cc < n; cc += blockDim.x) {
+            for (int cc = warp; cc < n; cc += 32) {
                 double s = 0.0;
-                for (int r = 0; r < n; r++) s += An[(size_t)cc * n + r] * An[(size_t)cc * n + r];
-                norms[cc] = sqrt(s);
+                for (int r = lane; r < n; r += 32) s += An[(size_t)cc * n + r] * An[(size_t)cc * n + r];
+                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+                if (lane == 0) norms[cc] = sqrt(s);
             }
-            const double* Wh = W + (size_t)h * n * n;
-            for (int i = tid; i < n; i += blockDim.x) {
+            if (tid < n) dc[tid] = cnew[tid] - ch[tid];
+            __syncthreads();
+            {
+                const int i = tid >> 3, part = tid & 7;
+                const double* Wh = W + (size_t)h * n * n;
                 double acc = 0.0;
-                for (int k = 0; k < n; k++) acc += Wh[(size_t)k * n + i] * (cnew[k] - ch[k]);
-                shift[i] = acc;
+                if (i < n)
+                    for (int k = part; k < n; k += 8) acc += Wh[(size_t)k * n + i] * dc[k];
+                acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+                acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+                acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+                if (part == 0 && i < n) shift[i] = acc;
             }
             __syncthreads();
-            for (int e = tid; e < n * n; e += blockDim.x) Ah[e] = An[e] / norms[e / n];
+            for (int cc = tid >> 7; cc < n; cc += 8) {
+                const int r = tid & 127;
+                if (r < n) Ah[(size_t)cc * n + r] = An[(size_t)cc * n + r] / norms[cc];
+            }
             for (int e = tid; e < m * n; e += blockDim.x) {
                 const int i = e % n;
                 const size_t idx = (size_t)h * m * n + e;
-                mu[idx] *= norms[i];
+                double mv = mu[idx] * norms[i];
                 beta[idx] /= (norms[i] * norms[i]);
-                mu[idx] -= shift[i];
+                mu[idx] = mv - shift[i];
             }
         } else {
             for (int e = tid; e < n * n; e += blockDim.x) Ah[e] = An[e];
@@ -388,16 +363,29 @@ __global__ void __launch_bounds__(256) k_reparm(int update_A, int do_reparm, dou
 }
 
 // ---------------------------------------------------------------------------
-// k_reduce: raw[h][e] = sum over clusters of partial[q][h][e], fixed order.
-// Replaces the block/device reductions of src/amica.cu:1618-1920.
-__global__ void k_reduce(const double* __restrict__ partial, double* __restrict__ raw, int nclusters,
-                         int M, int stride) {
+// k_reduce: raw[h][e] = sum over slots of partial[q][h][e], fixed order.  The
+// n x n block is carried only by every psi_step-th slot (the tensor-core E-step
+// keeps phi in one slot per cluster); when it already is phi it also goes
+// straight into the statistics vector.  Replaces the block/device reductions of
+// src/amica.cu:1618-1920.
+__global__ void k_reduce(const double* __restrict__ partial, double* __restrict__ raw,
+                         double* __restrict__ stats, int nslots, int M, int n, int m, int psi_step,
+                         int psi_is_phi) {
+    PartLayout PL{n, m};
+    StatLayout SL{n, m};
+    const int stride = PL.stride(), psi0 = PL.psi();
     const int64_t total = (int64_t)M * stride;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
          e += (int64_t)gridDim.x * blockDim.x) {
+        const int h = (int)(e / stride);
+        const int off = (int)(e - (int64_t)h * stride);
+        const bool in_psi = off >= psi0;
+        const int step = in_psi ? psi_step : 1;
         double s = 0.0;
-        for (int q = 0; q < nclusters; q++) s += partial[(size_t)q * total + e];
+#pragma unroll 4
+        for (int q = 0; q < nslots; q += step) s += partial[(size_t)q * total + e];
         raw[e] = s;
+        if (in_psi && psi_is_phi) stats[SL.base(h) + SL.phi() + (off - psi0)] = s;
     }
 }
 
@@ -425,14 +413,6 @@ __global__ void __launch_bounds__(kT) k_finalize(
         for (int k = 0; k < n; k++) acc += Ah[(size_t)k * n + i] * R[PL.cn() + k];
         S[SL.cn() + i] = acc;
         S[SL.s2() + i] = R[PL.s2() + i];
-    }
-    const double* Psi = R + PL.psi();
-    const double* gs = R + PL.gs();
-    const double* Wh = W + (size_t)h * n * n;
-    const double* ch = c + (size_t)h * n;
-    for (int e = tid; e < n * n; e += kT) {
-        const int i = e % n, k = e / n;
-        if (psi_is_phi) S[SL.phi() + (size_t)k * n + i] = Psi[e];
     }
     for (int e = tid; e < m * n; e += kT) {
         const size_t idx = (size_t)h * m * n + e;
@@ -471,11 +451,13 @@ __device__ double psi_series(double x) {
     return r;
 }
 
-// Per-model parameter updates (src/amica.cu:1995-2154) and the Newton /
-// natural-gradient matrix B (src/amica.cu:2155-2279, src/kernels.cu:961-1014).
-__global__ void __launch_bounds__(kT) k_mstep_params(
+// Per-model parameter updates (src/amica.cu:1995-2154) and the Newton
+// condition bflag (src/amica.cu:2155-2230).  One CTA of 1024 threads per model;
+// kappa, lambda, sigma2 and cnew go to `work` for the A update.
+constexpr int kMT = 1024;
+__global__ void __launch_bounds__(kMT) k_mstep_params(
     MCfg cf, const double* __restrict__ stats, Ctrl* ctrl, double* gm, double* alpha, double* mu,
-    double* beta, double* rho, double* work, double* B, int64_t* bflag, int* use_newton) {
+    double* beta, double* rho, double* work, int64_t* bflag, int* use_newton) {
     const int h = blockIdx.x, tid = threadIdx.x;
     const int n = cf.n, m = cf.m, mn = m * n;
     StatLayout SL{n, m};
@@ -487,15 +469,16 @@ __global__ void __launch_bounds__(kT) k_mstep_params(
     double* sig2 = kappa + 2 * n;
     double* cnew = kappa + 3 * n;
     __shared__ double sh[33];
+    __shared__ double ks[128];
     const double vsum = S[SL.vs()];
     const double ivs = 1.0 / vsum;
     if (tid == 0 && cf.update_gm) gm[h] = vsum / Tk;
-    for (int i = tid; i < n; i += kT) {
-        sig2[i] = S[SL.s2() + i] * ivs;
-        cnew[i] = S[SL.cn() + i] * ivs;
-    }
     // alpha = usum / vsum; then kappa / lambda with the new alpha and old mu
-    for (int i = tid; i < n; i += kT) {
+    if (tid < n) {
+        const int i = tid;
+        const double s2 = S[SL.s2() + i] * ivs;
+        sig2[i] = s2;
+        cnew[i] = S[SL.cn() + i] * ivs;
         double kap = 0.0, lam = 0.0;
         for (int j = 0; j < m; j++) {
             const int mi = j * n + i;
@@ -510,9 +493,10 @@ __global__ void __launch_bounds__(kT) k_mstep_params(
         }
         kappa[i] = kap;
         lambda[i] = lam;
+        ks[i] = kap * s2;
     }
     __syncthreads();
-    for (int mi = tid; mi < mn; mi += kT) {
+    for (int mi = tid; mi < mn; mi += kMT) {
         const size_t idx = (size_t)h * mn + mi;
         if (cf.update_mu) mu[idx] += S[SL.mix(kMn) + mi] / S[SL.mix(kMd) + mi];
         if (cf.update_beta) {
@@ -532,34 +516,16 @@ __global__ void __launch_bounds__(kT) k_mstep_params(
     if (!cf.update_A) return;
     // bflag: entries of (kappa sigma2)(kappa sigma2)^T that are <= 1, diagonal included
     double cnt = 0.0;
-    for (int e = tid; e < n * n; e += kT) {
-        const int r = e % n, cc = e / n;
-        const double d = (kappa[r] * sig2[r]) * (kappa[cc] * sig2[cc]);
-        if (d <= 1.0) cnt += 1.0;
+    {
+        const int r = tid & 127;
+        if (r < n)
+            for (int cc = tid >> 7; cc < n; cc += kMT / 128)
+                if (ks[r] * ks[cc] <= 1.0) cnt += 1.0;
     }
     cnt = block_sum(cnt, sh);
     const int64_t bf = (int64_t)cnt;
     const int newton = (bf == 0 && cf.do_newton && iter >= cf.newt_start_iter);
     if (tid == 0) { bflag[h] = bf; use_newton[h] = newton; }
-    const double* phi = S + SL.phi();
-    double* Bh = B + (size_t)h * n * n;
-    for (int e = tid; e < n * n; e += kT) {
-        const int r = e % n, cc = e / n;
-        const double prc = phi[(size_t)cc * n + r] * ivs;      // phi(r, c) / vsum
-        double v;
-        if (newton) {
-            if (r == cc) {
-                v = (1.0 - prc) / lambda[r];
-            } else {
-                const double pcr = phi[(size_t)r * n + cc] * ivs;
-                const double nom = -sig2[r] * kappa[cc];
-                v = (nom * (-prc) + (-pcr)) / ((kappa[r] * sig2[r]) * (kappa[cc] * sig2[cc]) - 1.0);
-            }
-        } else {
-            v = (r == cc ? 1.0 : 0.0) - prc;
-        }
-        Bh[e] = v;
-    }
 }
 
 // LL bookkeeping and the learning-rate schedule (src/amica.cu:1981-1993,
@@ -611,60 +577,6 @@ __global__ void k_ctrl(MCfg cf, const double* __restrict__ stats, Ctrl* ctrl,
         r.pad = 0;
         hist[iter - 1] = r;
     }
-}
-
-// A update and reparametrisation (src/amica.cu:2288-2447, src/kernels.cu:1023-1065).
-__global__ void __launch_bounds__(kT) k_mstep_A(MCfg cf, const Ctrl* __restrict__ ctrl, double* A,
-                                                double* Anew, const double* __restrict__ B,
-                                                const int* __restrict__ use_newton,
-                                                const double* __restrict__ W, double* c, double* mu,
-                                                double* beta, const double* __restrict__ work) {
-    const int h = blockIdx.x, tid = threadIdx.x;
-    const int n = cf.n, m = cf.m;
-    const double* cnew = work + (size_t)h * 4 * n + 3 * n;
-    double* ch = c + (size_t)h * n;
-    __shared__ double norms[256];
-    __shared__ double shift[256];
-    if (cf.update_A) {
-        double* Ah = A + (size_t)h * n * n;
-        double* An = Anew + (size_t)h * n * n;
-        const double* Bh = B + (size_t)h * n * n;
-        const double al = use_newton[h] ? ctrl->lrate : -ctrl->lrate;
-        for (int e = tid; e < n * n; e += kT) {
-            const int r = e % n, cc = e / n;
-            double acc = 0.0;
-            for (int k = 0; k < n; k++) acc += Ah[(size_t)k * n + r] * Bh[(size_t)cc * n + k];
-            An[e] = al * acc + Ah[e];
-        }
-        __syncthreads();
-        if (cf.do_reparm) {
-            for (int cc = tid; cc < n; cc += kT) {
-                double s = 0.0;
-                for (int r = 0; r < n; r++) s += An[(size_t)cc * n + r] * An[(size_t)cc * n + r];
-                norms[cc] = sqrt(s);
-            }
-            // W (cnew - c) with the W of the start of the iteration
-            const double* Wh = W + (size_t)h * n * n;
-            for (int i = tid; i < n; i += kT) {
-                double acc = 0.0;
-                for (int k = 0; k < n; k++) acc += Wh[(size_t)k * n + i] * (cnew[k] - ch[k]);
-                shift[i] = acc;
-            }
-            __syncthreads();
-            for (int e = tid; e < n * n; e += kT) Ah[e] = An[e] / norms[e / n];
-            for (int e = tid; e < m * n; e += kT) {
-                const int i = e % n;
-                const size_t idx = (size_t)h * m * n + e;
-                mu[idx] *= norms[i];
-                beta[idx] /= (norms[i] * norms[i]);
-                mu[idx] -= shift[i];
-            }
-        } else {
-            for (int e = tid; e < n * n; e += kT) Ah[e] = An[e];
-        }
-        __syncthreads();
-    }
-    for (int i = tid; i < n; i += kT) ch[i] = cnew[i];   // src/amica.cu:2456-2462
 }
 
 // Rejection pass (engine-defined; the reference has none): over kept samples,
@@ -766,19 +678,14 @@ static MCfg to_mcfg(const MStepCfgHost& h) {
 }
 
 cudaError_t launch_prep(const MStepBuffers& b, const MStepCfgHost& h, cudaStream_t st) {
-    if (h.n <= 128) {
-        const size_t smem = sizeof(double) * ((size_t)h.n * h.n + h.n);
-        cudaError_t e = cudaFuncSetAttribute(k_inverse_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-        k_inverse_smem<<<h.M, 1024, smem, st>>>(b.A, b.gm, h.ldetS, b.W, b.ldet, b.ltc64, h.n, b.err);
-        dim3 grid(h.M, (h.NP + 127) / 128);
-        k_derive<<<grid, 128, 0, st>>>(b.W, b.c, b.alpha, b.mu, b.beta, b.rho, b.Wf, b.wcf, b.mp, h.n,
-                                       h.m, h.NP);
-    } else {
-        k_prep<<<h.M, kT, 0, st>>>(b.A, b.c, b.alpha, b.mu, b.beta, b.rho, b.gm, h.ldetS, b.aug, b.W,
-                                   b.ldet, b.ltc64, b.Wf, b.wcf, b.mp, h.n, h.m, h.NP, b.err);
-    }
+    if (h.n > 128) return cudaErrorInvalidValue;
+    const size_t smem = sizeof(double) * (size_t)h.n * h.n;
+    cudaError_t e = cudaFuncSetAttribute(k_inverse_derive, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    k_inverse_derive<<<h.M, kInvThreads, smem, st>>>(b.A, b.c, b.alpha, b.mu, b.beta, b.rho, b.gm,
+                                                     h.ldetS, b.W, b.ldet, b.ltc64, b.Wf, b.wcf, b.mp,
+                                                     h.n, h.m, h.NP, b.err);
     return cudaGetLastError();
 }
 
@@ -789,14 +696,20 @@ cudaError_t launch_reduce_finalize(const MStepBuffers& b, const MStepCfgHost& h,
     const int64_t total = (int64_t)h.M * PL.stride();
     int grid = (int)((total + 255) / 256);
     if (grid > 4096) grid = 4096;
-    k_reduce<<<grid, 256, 0, st>>>(b.partial, b.raw, nclusters, h.M, PL.stride());
+    k_reduce<<<grid, 256, 0, st>>>(b.partial, b.raw, b.stats, nclusters, h.M, h.n, h.m,
+                                   h.psi_step > 0 ? h.psi_step : 1, h.psi_is_phi);
     k_finalize<<<h.M, kT, 0, st>>>(b.raw, b.W, b.A, b.c, b.beta, b.rho, b.ltc64, b.ctrl, b.stats,
                                    h.n, h.m, h.psi_is_phi);
     if (!h.psi_is_phi) {
         dim3 g((h.n + 31) / 32, (h.n + 31) / 32, h.M);
-        k_gemm64<<<g, 256, 0, st>>>(1, b.raw + PL.psi(), PL.stride(), b.W, (size_t)h.n * h.n,
-                                    b.stats + SL.base(0) + SL.phi(), SL.S(), b.raw + PL.gs(),
-                                    PL.stride(), b.c, nullptr, nullptr, h.n);
+        GemmArgs ga{};
+        ga.kind = 1; ga.n = h.n; ga.m = h.m;
+        ga.X = b.raw + PL.psi(); ga.strideX = PL.stride();
+        ga.Y = b.W; ga.strideY = (size_t)h.n * h.n;
+        ga.Out = b.stats + SL.base(0) + SL.phi(); ga.strideOut = SL.S();
+        ga.gs = b.raw + PL.gs(); ga.strideG = PL.stride();
+        ga.c = b.c;
+        k_gemm64<<<g, 256, 0, st>>>(ga);
     }
     return cudaGetLastError();
 }
@@ -804,15 +717,20 @@ cudaError_t launch_reduce_finalize(const MStepBuffers& b, const MStepCfgHost& h,
 cudaError_t launch_mstep(const MStepBuffers& b, const MStepCfgHost& h, const float* P_rel,
                          uint8_t* keep, int64_t T, cudaStream_t st) {
     const MCfg cf = to_mcfg(h);
-    k_mstep_params<<<h.M, kT, 0, st>>>(cf, b.stats, b.ctrl, b.gm, b.alpha, b.mu, b.beta, b.rho,
-                                       b.work, b.B, b.bflag, b.use_newton);
+    k_mstep_params<<<h.M, kMT, 0, st>>>(cf, b.stats, b.ctrl, b.gm, b.alpha, b.mu, b.beta, b.rho,
+                                        b.work, b.bflag, b.use_newton);
     k_ctrl<<<1, 32, 0, st>>>(cf, b.stats, b.ctrl, b.bflag, b.hist, b.hist_cap);
     if (h.update_A) {
         dim3 g((h.n + 31) / 32, (h.n + 31) / 32, h.M);
-        k_gemm64<<<g, 256, 0, st>>>(0, b.A, (size_t)h.n * h.n, b.B, (size_t)h.n * h.n, b.Anew,
-                                    (size_t)h.n * h.n, nullptr, 0, nullptr, b.use_newton, b.ctrl, h.n);
+        GemmArgs ga{};
+        ga.kind = 0; ga.n = h.n; ga.m = h.m;
+        ga.X = b.A; ga.strideX = (size_t)h.n * h.n;
+        ga.Out = b.Anew; ga.strideOut = (size_t)h.n * h.n;
+        ga.use_newton = b.use_newton; ga.ctrl = b.ctrl;
+        ga.stats = b.stats; ga.work = b.work;
+        k_gemm64<<<g, 256, 0, st>>>(ga);
     }
-    k_reparm<<<h.M, 256, 0, st>>>(h.update_A, h.do_reparm, b.A, b.Anew, b.W, b.c, b.mu, b.beta,
+    k_reparm<<<h.M, 1024, 0, st>>>(h.update_A, h.do_reparm, b.A, b.Anew, b.W, b.c, b.mu, b.beta,
                                   b.work, h.n, h.m);
     if (h.do_reject && P_rel && keep)
         k_reject<<<1, kT, 0, st>>>(cf, b.ctrl, P_rel, keep, T, b.chunk, b.hist, b.hist_cap, 0);
