@@ -76,7 +76,8 @@ __global__ void __launch_bounds__(kInvThreads, 1) k_inverse_derive(
     extern __shared__ double Ws[];                    // [n][n] row-major W_h, after elimination
     // colk[buf][g * 32 + i] = a(g + 4 i, k): each thread's rows are contiguous
     __shared__ __align__(16) double colk[2][128];
-    __shared__ double prow[2][128], cval[2][kInvGroups], pivs[128], wcs[128];
+    __shared__ double prow[2][128], pivs[128], wcs[128];
+    __shared__ unsigned long long cval[2][kInvGroups];   // bit pattern of |candidate| (0: none)
     __shared__ int cidx[2][kInvGroups], perm[128], pinv[128];
     const int h = blockIdx.x, tid = threadIdx.x;
     const int g = tid >> 7, col = tid & 127;
@@ -112,7 +113,7 @@ __global__ void __launch_bounds__(kInvThreads, 1) k_inverse_derive(
         if (lane == 0) {
             const int ib = 31 - (int)(key & 31u);
             const double pv = colk[buf][g * kInvRows + ib];
-            cval[buf][g] = key ? fabs(pv) : -1.0;
+            cval[buf][g] = key ? (unsigned long long)__double_as_longlong(fabs(pv)) : 0ull;
             cidx[buf][g] = key ? g + kInvGroups * ib : 0x7fffffff;
             cinv[buf][g] = key ? 1.0 / pv : 0.0;
         }
@@ -121,16 +122,17 @@ __global__ void __launch_bounds__(kInvThreads, 1) k_inverse_derive(
     for (int k = 0; k < n; k++) {
         const int buf = k & 1;
         __syncthreads();
-        double best = cval[buf][0];
+        // non-negative doubles order like their bit patterns
+        unsigned long long best = cval[buf][0];
         int p = cidx[buf][0];
         int gb = 0;
 #pragma unroll
         for (int q = 1; q < kInvGroups; q++) {
-            const double v = cval[buf][q];
+            const unsigned long long v = cval[buf][q];
             const int r = cidx[buf][q];
             if (v > best || (v == best && r < p)) { best = v; p = r; gb = q; }
         }
-        if (!(best > 0.0)) { bad = true; break; }    // same decision in every thread
+        if (best == 0ull) { bad = true; break; }     // same decision in every thread
         const int gp = p % kInvGroups, ip = p / kInvGroups;
         const double inv = cinv[buf][gb];
         if (g == gp) {
