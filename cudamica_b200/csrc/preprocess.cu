@@ -3,9 +3,10 @@
 // mean, cuBLAS Dsyrk and MAGMA dsyevd / dgesv / dgetrf).
 //
 //   mean      FP64 column sums, per-CTA partials reduced in fixed order
-//   C         X_c^T X_c / T in FP64 (register-blocked, per-CTA partials)
+//   C         X_c^T X_c / T in FP64 (8 x 8 register blocks, one CTA per SM)
 //   S         do_sphere 1: 2 C^{-1/2} from a parallel-ordered cyclic Jacobi
-//             eigendecomposition (one CTA, round-robin disjoint rotations);
+//             eigendecomposition (one CTA, round-robin disjoint rotations,
+//             matrix and eigenvectors in shared memory);
 //             do_sphere 2: diag(1/std) (std with T-1, src/kernels.cu:148-161);
 //             do_sphere 0: I
 //   ldetS     -log|det S| = -sum log of the eigen-scales
@@ -39,64 +40,6 @@ __global__ void k_mean(const double* __restrict__ part, int nblk, int n, int64_t
     }
 }
 
-// Partial covariance over one chunk: each thread owns an RB x RB block of C.
-template <int RB>
-__global__ void __launch_bounds__(256) k_cov(const float* __restrict__ x, int64_t T, int n,
-                                             const double* __restrict__ mean,
-                                             double* __restrict__ part) {
-    extern __shared__ double xs[];   // [32][n]
-    const int nb = (n + RB - 1) / RB;
-    const int64_t t0 = (int64_t)blockIdx.x * kChunk;
-    const int64_t t1 = t0 + kChunk < T ? t0 + kChunk : T;
-    // every thread handles up to ceil(nb*nb / 256) blocks
-    double acc[4][RB][RB];
-    const int nblocks = nb * nb;
-#pragma unroll
-    for (int q = 0; q < 4; q++)
-#pragma unroll
-        for (int a = 0; a < RB; a++)
-#pragma unroll
-            for (int b = 0; b < RB; b++) acc[q][a][b] = 0.0;
-    for (int64_t tb = t0; tb < t1; tb += 32) {
-        __syncthreads();
-        for (int e = threadIdx.x; e < 32 * n; e += blockDim.x) {
-            const int r = e / n, i = e % n;
-            const int64_t t = tb + r;
-            xs[e] = (t < t1) ? (double)x[t * n + i] - mean[i] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int blk = threadIdx.x + q * blockDim.x;
-            if (blk >= nblocks) break;
-            const int bi = (blk % nb) * RB, bk = (blk / nb) * RB;
-            for (int r = 0; r < 32; r++) {
-                double xi[RB], xk[RB];
-#pragma unroll
-                for (int a = 0; a < RB; a++) xi[a] = (bi + a < n) ? xs[r * n + bi + a] : 0.0;
-#pragma unroll
-                for (int b = 0; b < RB; b++) xk[b] = (bk + b < n) ? xs[r * n + bk + b] : 0.0;
-#pragma unroll
-                for (int a = 0; a < RB; a++)
-#pragma unroll
-                    for (int b = 0; b < RB; b++) acc[q][a][b] += xi[a] * xk[b];
-            }
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int blk = threadIdx.x + q * blockDim.x;
-        if (blk >= nblocks) break;
-        const int bi = (blk % nb) * RB, bk = (blk / nb) * RB;
-#pragma unroll
-        for (int a = 0; a < RB; a++)
-#pragma unroll
-            for (int b = 0; b < RB; b++)
-                if (bi + a < n && bk + b < n)
-                    part[(size_t)blockIdx.x * n * n + (size_t)(bk + b) * n + bi + a] = acc[q][a][b];
-    }
-}
-
 __global__ void k_cov_reduce(const double* __restrict__ part, int nblk, int n, int64_t T,
                              double* __restrict__ C) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -104,99 +47,6 @@ __global__ void k_cov_reduce(const double* __restrict__ part, int nblk, int n, i
     double s = 0.0;
     for (int b = 0; b < nblk; b++) s += part[(size_t)b * n * n + e];
     C[e] = s / (double)T;
-}
-
-// Parallel-ordered cyclic Jacobi: per round, n/2 disjoint (p,q) rotations from
-// a round-robin schedule; J^T A J applied as column then row updates.
-// a: n x n column-major (overwritten, becomes diagonal); V: eigenvectors.
-__global__ void __launch_bounds__(1024) k_jacobi(double* a, double* V, int n, double* evals) {
-    const int tid = threadIdx.x;
-    const int ne = (n % 2) ? n + 1 : n;   // pad to even with a dummy index
-    __shared__ double cs[256], sn[256];
-    __shared__ int pp[256], qq[256];
-    __shared__ double red[32];
-    __shared__ int stop;
-    for (int e = tid; e < n * n; e += blockDim.x) V[e] = ((e % n) == (e / n)) ? 1.0 : 0.0;
-    __syncthreads();
-    for (int sweep = 0; sweep < 40; sweep++) {
-        // convergence: off-diagonal vs Frobenius
-        double off = 0.0, fro = 0.0;
-        for (int e = tid; e < n * n; e += blockDim.x) {
-            const double v = a[e];
-            fro += v * v;
-            if ((e % n) != (e / n)) off += v * v;
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            off += __shfl_xor_sync(0xffffffffu, off, o);
-            fro += __shfl_xor_sync(0xffffffffu, fro, o);
-        }
-        if (tid % 32 == 0) { red[tid / 32] = off; }
-        __syncthreads();
-        if (tid == 0) {
-            double s = 0.0;
-            for (int w = 0; w < (int)(blockDim.x / 32); w++) s += red[w];
-            red[0] = s;
-        }
-        __syncthreads();
-        const double offt = red[0];
-        __syncthreads();
-        if (tid % 32 == 0) red[tid / 32] = fro;
-        __syncthreads();
-        if (tid == 0) {
-            double s = 0.0;
-            for (int w = 0; w < (int)(blockDim.x / 32); w++) s += red[w];
-            stop = (offt <= 1e-30 * s);
-        }
-        __syncthreads();
-        if (stop) break;
-        for (int round = 0; round < ne - 1; round++) {
-            const int half = ne / 2;
-            for (int k = tid; k < half; k += blockDim.x) {
-                auto pos = [&](int j) { return j == 0 ? 0 : 1 + ((j - 1 + round) % (ne - 1)); };
-                int p = pos(k), q = pos(ne - 1 - k);
-                if (p > q) { int t = p; p = q; q = t; }
-                double c = 1.0, s = 0.0;
-                if (q < n) {
-                    const double apq = a[(size_t)q * n + p];
-                    if (fabs(apq) >= 1e-300) {
-                        const double app = a[(size_t)p * n + p], aqq = a[(size_t)q * n + q];
-                        const double th = (aqq - app) / (2.0 * apq);
-                        const double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
-                        c = 1.0 / sqrt(t * t + 1.0);
-                        s = t * c;
-                    }
-                }
-                pp[k] = p; qq[k] = q; cs[k] = c; sn[k] = s;
-            }
-            __syncthreads();
-            // columns p, q (and V)
-            for (int e = tid; e < half * n; e += blockDim.x) {
-                const int k = e / n, r = e % n;
-                const int p = pp[k], q = qq[k];
-                if (q >= n || sn[k] == 0.0) continue;
-                const double c = cs[k], s = sn[k];
-                const double arp = a[(size_t)p * n + r], arq = a[(size_t)q * n + r];
-                a[(size_t)p * n + r] = c * arp - s * arq;
-                a[(size_t)q * n + r] = s * arp + c * arq;
-                const double vrp = V[(size_t)p * n + r], vrq = V[(size_t)q * n + r];
-                V[(size_t)p * n + r] = c * vrp - s * vrq;
-                V[(size_t)q * n + r] = s * vrp + c * vrq;
-            }
-            __syncthreads();
-            // rows p, q
-            for (int e = tid; e < half * n; e += blockDim.x) {
-                const int k = e / n, col = e % n;
-                const int p = pp[k], q = qq[k];
-                if (q >= n || sn[k] == 0.0) continue;
-                const double c = cs[k], s = sn[k];
-                const double apc = a[(size_t)col * n + p], aqc = a[(size_t)col * n + q];
-                a[(size_t)col * n + p] = c * apc - s * aqc;
-                a[(size_t)col * n + q] = s * apc + c * aqc;
-            }
-            __syncthreads();
-        }
-    }
-    for (int i = tid; i < n; i += blockDim.x) evals[i] = a[(size_t)i * n + i];
 }
 
 // S = V diag(2/sqrt(d)) V^T (do_sphere 1), diag(1/std) (2) or I (0); ldetS.
@@ -268,26 +118,254 @@ __device__ __forceinline__ float round_tf32(float v) {
     return __uint_as_float(r);
 }
 
-__global__ void __launch_bounds__(256) k_apply_sphere(const float* __restrict__ x, int64_t T, int n,
-                                                      const double* __restrict__ mean,
-                                                      const double* __restrict__ S,
-                                                      float* __restrict__ xo, int ldx, int tf32) {
-    extern __shared__ double xc[];   // [16][n]
-    const int64_t t0 = (int64_t)blockIdx.x * 16;
-    for (int e = threadIdx.x; e < 16 * n; e += blockDim.x) {
-        const int r = e / n, k = e % n;
-        const int64_t t = t0 + r;
-        xc[e] = (t < T) ? (double)x[t * n + k] - mean[k] : 0.0;
+// Partial covariance: one persistent CTA per SM over a contiguous sample range;
+// thread (bi, bk) owns the 8 x 8 block C[8 bi .. 8 bi + 7][8 bk .. 8 bk + 7] in
+// registers (n <= 128: 16 x 16 blocks, 256 threads).  Samples are staged 32 at
+// a time, centred, in shared memory.
+constexpr int kCovRows = 32;
+__global__ void __launch_bounds__(256, 1) k_cov8(const float* __restrict__ x, int64_t T, int n,
+                                                 int64_t chunk, const double* __restrict__ mean,
+                                                 double* __restrict__ part) {
+    __shared__ __align__(16) double xs[kCovRows][128];
+    const int bi = threadIdx.x & 15, bk = threadIdx.x >> 4;
+    const int64_t t0 = (int64_t)blockIdx.x * chunk;
+    const int64_t t1 = t0 + chunk < T ? t0 + chunk : T;
+    double acc[8][8];
+#pragma unroll
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int b = 0; b < 8; b++) acc[a][b] = 0.0;
+    for (int64_t tb = t0; tb < t1; tb += kCovRows) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < kCovRows * 128; e += 256) {
+            const int r = e >> 7, i = e & 127;
+            const int64_t t = tb + r;
+            xs[r][i] = (t < t1 && i < n) ? (double)x[t * n + i] - mean[i] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 2
+        for (int r = 0; r < kCovRows; r++) {
+            double xi[8], xk[8];
+#pragma unroll
+            for (int a = 0; a < 8; a += 2) {
+                const double2 u = *reinterpret_cast<const double2*>(&xs[r][8 * bi + a]);
+                const double2 w = *reinterpret_cast<const double2*>(&xs[r][8 * bk + a]);
+                xi[a] = u.x; xi[a + 1] = u.y; xk[a] = w.x; xk[a + 1] = w.y;
+            }
+#pragma unroll
+            for (int a = 0; a < 8; a++)
+#pragma unroll
+                for (int b = 0; b < 8; b++) acc[a][b] = fma(xi[a], xk[b], acc[a][b]);
+        }
     }
+#pragma unroll
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const int i = 8 * bi + a, k = 8 * bk + b;
+            if (i < n && k < n) part[(size_t)blockIdx.x * n * n + (size_t)k * n + i] = acc[a][b];
+        }
+}
+
+// Parallel-ordered cyclic Jacobi eigendecomposition of the symmetric n x n
+// matrix C (n <= 128), one CTA, everything in shared memory: the upper
+// triangle of the working matrix packed by columns and the eigenvector matrix
+// V.  A round applies n/2 disjoint rotations (p_k, q_k) of the round-robin
+// schedule at once.  Since J^T A J only mixes rows {p_K, q_K} with columns
+// {p_L, q_L}, each 2 x 2 block (K, L), K <= L, is transformed independently by
+// the thread that owns it; V <- V J rotates column pairs.  Sweeps stop when the
+// off-diagonal energy is below 1e-30 of the total.
+__device__ __forceinline__ int pk_idx(int i, int j) {   // i <= j
+    return (j * (j + 1)) / 2 + i;
+}
+__device__ __forceinline__ int pk_sym(int i, int j) { return i <= j ? pk_idx(i, j) : pk_idx(j, i); }
+
+constexpr int kJacThreads = 1024;
+__global__ void __launch_bounds__(kJacThreads, 1) k_jacobi_smem(const double* __restrict__ C,
+                                                                double* __restrict__ Vout,
+                                                                double* __restrict__ evals, int n) {
+    extern __shared__ __align__(16) double jsm[];
+    const int np = (n * (n + 1)) / 2;
+    double* ap = jsm;                                   // packed upper triangle
+    double* V = jsm + ((np + 1) & ~1);                  // n x n, column-major
+    __shared__ double cs[64], sn[64];
+    __shared__ int pp[64], qq[64];
+    __shared__ unsigned short blkKL[64 * 65 / 2];   // (K << 8) | L for the 2 x 2 blocks, K <= L
+    __shared__ double red[32];
+    __shared__ int stop;
+    const int tid = threadIdx.x;
+    const int ne = n + (n & 1), half = ne / 2;
+    const int nblk = half * (half + 1) / 2;
+    for (int e = tid; e < n * n; e += kJacThreads) {
+        const int r = e % n, c = e / n;
+        if (r <= c) ap[pk_idx(r, c)] = C[e];
+        V[e] = (r == c) ? 1.0 : 0.0;
+    }
+    if (tid < half)
+        for (int K = 0; K <= tid; K++) blkKL[tid * (tid + 1) / 2 + K] = (unsigned short)((K << 8) | tid);
     __syncthreads();
-    for (int e = threadIdx.x; e < 16 * ldx; e += blockDim.x) {
-        const int r = e / ldx, i = e % ldx;
-        const int64_t t = t0 + r;
-        if (t >= T) continue;
-        double acc = 0.0;
-        if (i < n)
-            for (int k = 0; k < n; k++) acc += S[(size_t)k * n + i] * xc[r * n + k];
-        xo[t * ldx + i] = tf32 ? round_tf32((float)acc) : (float)acc;
+    for (int sweep = 0; sweep < 40; sweep++) {
+        double off = 0.0, tot = 0.0;
+        for (int e = tid; e < np; e += kJacThreads) {
+            // column j of the packed triangle holds rows 0..j; the last one is diagonal
+            int j = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+            while (pk_idx(0, j + 1) <= e) j++;
+            while (pk_idx(0, j) > e) j--;
+            const double v = ap[e];
+            const bool diag = (e - pk_idx(0, j)) == j;
+            tot += diag ? v * v : 2.0 * v * v;
+            off += diag ? 0.0 : 2.0 * v * v;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            off += __shfl_xor_sync(0xffffffffu, off, o);
+            tot += __shfl_xor_sync(0xffffffffu, tot, o);
+        }
+        if ((tid & 31) == 0) red[tid >> 5] = off;
+        __syncthreads();
+        if (tid == 0) {
+            double s = 0.0;
+            for (int w = 0; w < kJacThreads / 32; w++) s += red[w];
+            red[0] = s;
+        }
+        __syncthreads();
+        const double offt = red[0];
+        __syncthreads();
+        if ((tid & 31) == 0) red[tid >> 5] = tot;
+        __syncthreads();
+        if (tid == 0) {
+            double s = 0.0;
+            for (int w = 0; w < kJacThreads / 32; w++) s += red[w];
+            stop = (offt <= 1e-30 * s);
+        }
+        __syncthreads();
+        if (stop) break;
+        for (int round = 0; round < ne - 1; round++) {
+            if (tid < half) {
+                auto pos = [&](int j) { return j == 0 ? 0 : 1 + ((j - 1 + round) % (ne - 1)); };
+                int p = pos(tid), q = pos(ne - 1 - tid);
+                if (p > q) { const int t = p; p = q; q = t; }
+                double c = 1.0, s = 0.0;
+                if (q < n) {
+                    const double apq = ap[pk_idx(p, q)];
+                    if (fabs(apq) >= 1e-300) {
+                        const double app = ap[pk_idx(p, p)], aqq = ap[pk_idx(q, q)];
+                        const double th = (aqq - app) / (2.0 * apq);
+                        const double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+                        c = 1.0 / sqrt(t * t + 1.0);
+                        s = t * c;
+                    }
+                }
+                pp[tid] = p; qq[tid] = q; cs[tid] = c; sn[tid] = s;
+            }
+            __syncthreads();
+            // A <- J^T A J, one 2 x 2 block (K <= L) per work item
+            for (int e = tid; e < nblk; e += kJacThreads) {
+                const int K = blkKL[e] >> 8, L = blkKL[e] & 0xff;
+                const int pK = pp[K], qK = qq[K], pL = pp[L], qL = qq[L];
+                const double cK = cs[K], sK = sn[K], cL = cs[L], sL = sn[L];
+                if (K == L) {
+                    if (qK < n && sK != 0.0) {
+                        const double app = ap[pk_idx(pK, pK)], aqq = ap[pk_idx(qK, qK)];
+                        const double apq = ap[pk_idx(pK, qK)];
+                        ap[pk_idx(pK, pK)] = cK * cK * app - 2.0 * cK * sK * apq + sK * sK * aqq;
+                        ap[pk_idx(qK, qK)] = sK * sK * app + 2.0 * cK * sK * apq + cK * cK * aqq;
+                        ap[pk_idx(pK, qK)] = 0.0;
+                    }
+                    continue;
+                }
+                if (sK == 0.0 && sL == 0.0) continue;
+                const bool hq = qK < n, hqL = qL < n;
+                const double b11 = ap[pk_sym(pK, pL)];
+                const double b12 = hqL ? ap[pk_sym(pK, qL)] : 0.0;
+                const double b21 = hq ? ap[pk_sym(qK, pL)] : 0.0;
+                const double b22 = (hq && hqL) ? ap[pk_sym(qK, qL)] : 0.0;
+                // B J_L (columns), then J_K^T (rows); J = [[c, s], [-s, c]]
+                const double d11 = cL * b11 - sL * b12, d12 = sL * b11 + cL * b12;
+                const double d21 = cL * b21 - sL * b22, d22 = sL * b21 + cL * b22;
+                ap[pk_sym(pK, pL)] = cK * d11 - sK * d21;
+                if (hqL) ap[pk_sym(pK, qL)] = cK * d12 - sK * d22;
+                if (hq) ap[pk_sym(qK, pL)] = sK * d11 + cK * d21;
+                if (hq && hqL) ap[pk_sym(qK, qL)] = sK * d12 + cK * d22;
+            }
+            // V <- V J: 16 threads per rotation, rows r = lane16, lane16 + 16, ...
+            for (int k = tid >> 4; k < half; k += kJacThreads / 16) {
+                const int p = pp[k], q = qq[k];
+                const double s = sn[k];
+                if (q >= n || s == 0.0) continue;
+                const double c = cs[k];
+                for (int r = tid & 15; r < n; r += 16) {
+                    const double vp = V[(size_t)p * n + r], vq = V[(size_t)q * n + r];
+                    V[(size_t)p * n + r] = c * vp - s * vq;
+                    V[(size_t)q * n + r] = s * vp + c * vq;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int e = tid; e < n * n; e += kJacThreads) Vout[e] = V[e];
+    for (int i = tid; i < n; i += kJacThreads) evals[i] = ap[pk_idx(i, i)];
+}
+
+// x_out[t][i] = sum_k S(i,k) (x[t][k] - mean[k]) in FP64, rounded once to FP32
+// (padded channels zero).  Persistent CTAs of 512 threads; S staged in shared
+// memory; a thread computes 4 channels x 4 samples of a 64-sample tile.
+constexpr int kSphTile = 64;
+__global__ void __launch_bounds__(512, 1) k_apply_sphere8(const float* __restrict__ x, int64_t T, int n,
+                                                          const double* __restrict__ mean,
+                                                          const double* __restrict__ S,
+                                                          float* __restrict__ xo, int ldx, int tf32) {
+    extern __shared__ __align__(16) double ssm[];
+    double* Ss = ssm;
+    double* xc = ssm + 128 * 128;
+    constexpr int XL = 129;
+    for (int e = threadIdx.x; e < 128 * 128; e += 512) {
+        const int k = e >> 7, i = e & 127;
+        Ss[e] = (i < n && k < n) ? S[(size_t)k * n + i] : 0.0;
+    }
+    const int ib = threadIdx.x & 31, tb = threadIdx.x >> 5;     // channels 4 ib.., samples 4 tb..
+    const int64_t ntile = (T + kSphTile - 1) / kSphTile;
+    for (int64_t tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+        const int64_t t0 = tile * kSphTile;
+        __syncthreads();
+        for (int e = threadIdx.x; e < kSphTile * 128; e += 512) {
+            const int r = e >> 7, k = e & 127;
+            const int64_t t = t0 + r;
+            xc[r * XL + k] = (t < T && k < n) ? (double)x[t * n + k] - mean[k] : 0.0;
+        }
+        __syncthreads();
+        double acc[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+#pragma unroll 4
+        for (int k = 0; k < n; k++) {
+            double s4[4], x4[4];
+#pragma unroll
+            for (int b = 0; b < 4; b += 2) {
+                const double2 v = *reinterpret_cast<const double2*>(&Ss[k * 128 + 4 * ib + b]);
+                s4[b] = v.x; s4[b + 1] = v.y;
+            }
+#pragma unroll
+            for (int a = 0; a < 4; a++) x4[a] = xc[(4 * tb + a) * XL + k];
+#pragma unroll
+            for (int a = 0; a < 4; a++)
+#pragma unroll
+                for (int b = 0; b < 4; b++) acc[a][b] = fma(s4[b], x4[a], acc[a][b]);
+        }
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+            const int64_t t = t0 + 4 * tb + a;
+            if (t >= T) continue;
+#pragma unroll
+            for (int b = 0; b < 4; b++) {
+                const int i = 4 * ib + b;
+                if (i < ldx) {
+                    const float v = (i < n) ? (float)acc[a][b] : 0.f;
+                    xo[t * ldx + i] = tf32 ? round_tf32(v) : v;
+                }
+            }
+        }
     }
 }
 
@@ -311,10 +389,16 @@ namespace amica {
 cudaError_t launch_preprocess(const float* raw, int64_t T, int n, int do_sphere, double* means,
                               double* cov, double* sphere, double* evwork, double* ldetS_dev,
                               float* x, int ldx, int tf32, cudaStream_t st) {
-    if (n > 256) return cudaErrorInvalidValue;
+    if (n > 128 || ldx > 128) return cudaErrorInvalidValue;
     const int nblk = (int)((T + kChunk - 1) / kChunk);
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int ncov = nsm;
+    const int64_t chunk = ((T + ncov - 1) / ncov + kCovRows - 1) / kCovRows * kCovRows;
     double* part = nullptr;
-    const size_t part_len = (size_t)nblk * n * n > (size_t)nblk * n ? (size_t)nblk * n * n : (size_t)nblk * n;
+    size_t part_len = (size_t)nblk * n;
+    if ((size_t)ncov * n * n > part_len) part_len = (size_t)ncov * n * n;
     cudaError_t e = cudaMallocAsync(&part, sizeof(double) * part_len, st);
     if (e != cudaSuccess) return e;
     k_colsum<<<nblk, 256, 0, st>>>(raw, T, n, part);
@@ -323,26 +407,22 @@ cudaError_t launch_preprocess(const float* raw, int64_t T, int n, int do_sphere,
     double* ev = evwork + (size_t)n * n;
     double* var = ev + n;
     if (do_sphere == 1) {
-        const int RB = 4;
-        const int nb = (n + RB - 1) / RB;
-        if (nb * nb > 4 * 256) { cudaFreeAsync(part, st); return cudaErrorInvalidValue; }
-        const size_t smem = sizeof(double) * 32 * n;
-        e = cudaFuncSetAttribute(k_cov<RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_cov8<<<ncov, 256, 0, st>>>(raw, T, n, chunk, means, part);
+        k_cov_reduce<<<(n * n + 255) / 256, 256, 0, st>>>(part, ncov, n, T, cov);
+        const size_t jsmem = sizeof(double) * (size_t)((((n * (n + 1)) / 2 + 1) & ~1) + n * n);
+        e = cudaFuncSetAttribute(k_jacobi_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)jsmem);
         if (e != cudaSuccess) { cudaFreeAsync(part, st); return e; }
-        k_cov<RB><<<nblk, 256, smem, st>>>(raw, T, n, means, part);
-        k_cov_reduce<<<(n * n + 255) / 256, 256, 0, st>>>(part, nblk, n, T, cov);
-        e = cudaMemcpyAsync(evwork + 2 * (size_t)n * n, cov, sizeof(double) * n * n,
-                            cudaMemcpyDeviceToDevice, st);
-        if (e != cudaSuccess) { cudaFreeAsync(part, st); return e; }
-        k_jacobi<<<1, 1024, 0, st>>>(evwork + 2 * (size_t)n * n, V, n, ev);
+        k_jacobi_smem<<<1, kJacThreads, jsmem, st>>>(cov, V, ev, n);
     } else if (do_sphere == 2) {
         k_var<<<n, 256, 0, st>>>(raw, T, n, means, var);
     }
     k_sphere<<<(n * n + 255) / 256, 256, 0, st>>>(V, ev, var, n, do_sphere, sphere, ldetS_dev);
-    const size_t smem2 = sizeof(double) * 16 * n;
-    e = cudaFuncSetAttribute(k_apply_sphere, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);
+    const size_t smem2 = sizeof(double) * (128 * 128 + kSphTile * 129);
+    e = cudaFuncSetAttribute(k_apply_sphere8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);
     if (e != cudaSuccess) { cudaFreeAsync(part, st); return e; }
-    k_apply_sphere<<<(unsigned)((T + 15) / 16), 256, smem2, st>>>(raw, T, n, means, sphere, x, ldx, tf32);
+    const int64_t ntile = (T + kSphTile - 1) / kSphTile;
+    const int gsph = (int)(ntile < nsm ? ntile : nsm);
+    k_apply_sphere8<<<gsph, 512, smem2, st>>>(raw, T, n, means, sphere, x, ldx, tf32);
     cudaFreeAsync(part, st);
     return cudaGetLastError();
 }
