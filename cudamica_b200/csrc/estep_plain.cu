@@ -19,6 +19,7 @@
 #include <cstdio>
 
 #include "common.cuh"
+#include "density.cuh"
 
 namespace cg = cooperative_groups;
 using namespace amica;
@@ -42,8 +43,8 @@ struct PlainShape {
     static constexpr int RI = NP / 16;
     static constexpr int RK = NP / 16;
     static constexpr int LLD = NP + 1;              // padded row of the lse tile
-    static constexpr size_t smem_floats =
-        (size_t)NP * WLD + (size_t)kS * XLD + (size_t)kS * NP + (size_t)kS * LLD + 2 * kS + 2 * kS;
+    static constexpr size_t smem_floats = (size_t)NP * WLD + (size_t)kS * XLD + (size_t)kS * NP +
+                                          (size_t)kS * LLD + (size_t)kS * LLD + 2 * kS + 2 * kS;
 };
 
 template <int NP, int MM>
@@ -53,8 +54,9 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     float* Wt = sm;                                   // [NP][WLD]  Wt[k][i] = W[i][k]
     float* xs = Wt + NP * Sh::WLD;                    // [S][XLD]
     float* bs = xs + kS * Sh::XLD;                    // [S][NP]    (W x)_i per sample
-    float* gs = bs + kS * NP;                         // [S][NP] g; as lse: [S][LLD]
-    float* slot = gs + kS * Sh::LLD;                  // [2][S]     cluster-visible L_h(t)
+    float* gs = bs + kS * NP;                         // [S][NP] g; its region is [S][LLD]
+    float* lse = gs + kS * Sh::LLD;                   // [S][LLD]   log-sum-exp over mixtures
+    float* slot = lse + kS * Sh::LLD;                 // [2][S]     cluster-visible L_h(t)
     float* vS = slot + 2 * kS;                        // [S]        v_h(t) (0 if not used)
 
     cg::cluster_group cluster = cg::this_cluster();
@@ -75,21 +77,40 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     const int ch = tid % NP;            // density-phase channel
     const int grp = tid / NP;           // density-phase sample group
     const bool ch_ok = ch < n;
-    float ps[MM], po[MM], pc[MM], pr[MM];
+    // mixtures (0,1), (2,3) as float2 pairs, an odd last one as a scalar
+    constexpr int NPR = MM / 2;
+    constexpr bool kOdd = (MM & 1) != 0;
+    constexpr int NPRA = NPR > 0 ? NPR : 1;
+    float pr[MM];
+    MixV<float2> P2[NPRA];
+    MixV<float> P1;
 #pragma unroll
     for (int j = 0; j < MM; j++) {
-        MixParam q = a.mp[((size_t)h * MM + j) * NP + ch];
-        ps[j] = q.s; po[j] = q.off; pc[j] = q.cl2; pr[j] = q.rho;
+        const MixParam q = a.mp[((size_t)h * MM + j) * NP + ch];
+        pr[j] = q.rho;
+        if (j < 2 * NPR) {
+            float2* f[5] = {&P2[j / 2].s, &P2[j / 2].npo, &P2[j / 2].pc, &P2[j / 2].pr, &P2[j / 2].sr};
+            const float vals[5] = {q.s, -q.off, q.cl2, q.rho, q.s * q.rho};
+#pragma unroll
+            for (int e = 0; e < 5; e++) {
+                if (j & 1) f[e]->y = vals[e];
+                else f[e]->x = vals[e];
+            }
+        } else {
+            P1.s = q.s; P1.npo = -q.off; P1.pc = q.cl2; P1.pr = q.rho; P1.sr = q.s * q.rho;
+        }
     }
     const float wci = a.wc[(size_t)h * NP + ch];
     float ltc[kMaxModels];
 #pragma unroll
     for (int q = 0; q < kMaxModels; q++) ltc[q] = (q < M) ? (float)(a.ltc64[q] - a.ltc64[0]) : 0.f;
 
-    // FP64 running sums for this thread's channel
-    double dUs[MM], dKn[MM], dLn[MM], dMn[MM], dMd[MM], dBd[MM], dRn[MM];
+    // FP64 running sums for this thread's channel: A0..A6 of dens_acc per mixture
+    double dA[7][MM];
 #pragma unroll
-    for (int j = 0; j < MM; j++) dUs[j] = dKn[j] = dLn[j] = dMn[j] = dMd[j] = dBd[j] = dRn[j] = 0.0;
+    for (int k = 0; k < 7; k++)
+#pragma unroll
+        for (int j = 0; j < MM; j++) dA[k][j] = 0.0;
     double dCn = 0.0, dS2 = 0.0, dGs = 0.0;
     double dLL = 0.0, dVs = 0.0;   // per-sample threads (tid < S)
     float psi[Sh::RI][Sh::RK];
@@ -143,24 +164,22 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
         }
         __syncthreads();
         // ---- phase 1: per (channel, sample) log-sum-exp over mixtures (log2 units)
-        float* lse = gs;
 #pragma unroll 4
         for (int r = 0; r < Sh::SUB; r++) {
             const int t = grp * Sh::SUB + r;
             const float bx = bs[t * NP + ch];
-            float q[MM], qmax = -INFINITY;
+            float q[MM];
 #pragma unroll
-            for (int j = 0; j < MM; j++) {
-                float y = fmaf(ps[j], bx, -po[j]);
-                float ay = fmaxf(fabsf(y), kTinyAbs);
-                float p = ptx_ex2(pr[j] * ptx_lg2(ay));
-                q[j] = fmaf(-p, kLog2e, pc[j]);
-                qmax = fmaxf(qmax, q[j]);
+            for (int qq = 0; qq < NPR; qq++) {
+                float2 L2;
+                const float2 q2 = dens_q(P2[qq], bx, L2);
+                q[2 * qq] = q2.x; q[2 * qq + 1] = q2.y;
             }
-            float se = 0.f;
-#pragma unroll
-            for (int j = 0; j < MM; j++) se += ptx_ex2(q[j] - qmax);
-            lse[t * Sh::LLD + ch] = ch_ok ? qmax + ptx_lg2(se) : 0.f;
+            if constexpr (kOdd) {
+                float L2;
+                q[MM - 1] = dens_q(P1, bx, L2);
+            }
+            lse[t * Sh::LLD + ch] = ch_ok ? lse2<MM>(q) : 0.f;
         }
         __syncthreads();
         // ---- Lt_h(t): channel sum in fixed order, published for the cluster
@@ -204,64 +223,43 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
         __syncthreads();
         // ---- phase 2: responsibilities, score function and sufficient statistics
         {
-            float fUs[MM], fKn[MM], fLn[MM], fMn[MM], fMd[MM], fBd[MM], fRn[MM];
+            float2 fP[NPRA][7];
+            float fS1[7];
 #pragma unroll
-            for (int j = 0; j < MM; j++) fUs[j] = fKn[j] = fLn[j] = fMn[j] = fMd[j] = fBd[j] = fRn[j] = 0.f;
+            for (int k = 0; k < 7; k++) {
+#pragma unroll
+                for (int qq = 0; qq < NPRA; qq++) fP[qq][k] = make_float2(0.f, 0.f);
+                fS1[k] = 0.f;
+            }
             float fCn = 0.f, fS2 = 0.f, fGs = 0.f;
 #pragma unroll 2
             for (int r = 0; r < Sh::SUB; r++) {
                 const int t = grp * Sh::SUB + r;
                 const float v = vS[t];
                 const float bx = bs[t * NP + ch];
-                float y[MM], L2[MM], p[MM], q[MM], qmax = -INFINITY;
+                const float nl = -lse[t * Sh::LLD + ch];
+                float2 g2 = make_float2(0.f, 0.f);
+                float g1 = 0.f;
 #pragma unroll
-                for (int j = 0; j < MM; j++) {
-                    y[j] = fmaf(ps[j], bx, -po[j]);
-                    float ay = fmaxf(fabsf(y[j]), kTinyAbs);
-                    L2[j] = ptx_lg2(ay);
-                    p[j] = ptx_ex2(pr[j] * L2[j]);
-                    q[j] = fmaf(-p[j], kLog2e, pc[j]);
-                    qmax = fmaxf(qmax, q[j]);
-                }
-                float e[MM], se = 0.f;
-#pragma unroll
-                for (int j = 0; j < MM; j++) { e[j] = ptx_ex2(q[j] - qmax); se += e[j]; }
-                const float vr = v * ptx_rcp(se);
-                float g = 0.f;
-#pragma unroll
-                for (int j = 0; j < MM; j++) {
-                    const float u = e[j] * vr;
-                    const float ay = fmaxf(fabsf(y[j]), kTinyAbs);
-                    const float ri = ptx_rcp(ay);
-                    const float pm1 = p[j] * ri;                 // |y|^(rho-1)
-                    const float fp = copysignf(pr[j] * pm1, y[j]);
-                    const float ufp = u * fp;
-                    g = fmaf(ps[j], ufp, g);
-                    fUs[j] += u;
-                    fKn[j] = fmaf(ufp, fp, fKn[j]);
-                    const float lv = fmaf(fp, y[j], -1.f);
-                    fLn[j] = fmaf(u * lv, lv, fLn[j]);
-                    fMn[j] += ufp;
-                    if (pr[j] <= 2.f || a.grad_mode) {
-                        fMd[j] = fmaf(ufp, copysignf(ri, y[j]), fMd[j]);
-                        fBd[j] = fmaf(ufp, y[j], fBd[j]);
-                    } else {
-                        fMd[j] = fmaf(ufp, fp, fMd[j]);
-                        fBd[j] = fmaf(u, p[j], fBd[j]);
-                    }
-                    if (a.update_rho) fRn[j] = fmaf(u * p[j], pr[j] * L2[j] * kLn2, fRn[j]);
-                }
+                for (int qq = 0; qq < NPR; qq++)
+                    dens_acc<float2, false>(P2[qq], bx, make_float2(0.f, 0.f), nl, v, fP[qq], g2);
+                if constexpr (kOdd) dens_acc<float, false>(P1, bx, 0.f, nl, v, fS1, g1);
+                const float g = (g2.x + g2.y) + g1;
                 const float bb = bx - wci;
                 fCn = fmaf(v, bb, fCn);          // sum v b; cnew = A sum(v b) / vsum + c
                 fS2 = fmaf(v * bb, bb, fS2);
-                fGs += g;
+                fGs += ch_ok ? g : 0.f;
                 gs[t * NP + ch] = ch_ok ? g : 0.f;
             }
             if (ch_ok) {
 #pragma unroll
-                for (int j = 0; j < MM; j++) {
-                    dUs[j] += fUs[j]; dKn[j] += fKn[j]; dLn[j] += fLn[j]; dMn[j] += fMn[j];
-                    dMd[j] += fMd[j]; dBd[j] += fBd[j]; dRn[j] += fRn[j];
+                for (int k = 0; k < 7; k++) {
+#pragma unroll
+                    for (int qq = 0; qq < NPR; qq++) {
+                        dA[k][2 * qq] += fP[qq][k].x;
+                        dA[k][2 * qq + 1] += fP[qq][k].y;
+                    }
+                    if constexpr (kOdd) dA[k][MM - 1] += fS1[k];
                 }
                 dCn += fCn; dS2 += fS2; dGs += fGs;
             }
@@ -295,9 +293,10 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     double vals[NACC];
 #pragma unroll
     for (int j = 0; j < MM; j++) {
-        vals[0 * MM + j] = dUs[j]; vals[1 * MM + j] = dKn[j]; vals[2 * MM + j] = dLn[j];
-        vals[3 * MM + j] = dMn[j]; vals[4 * MM + j] = dMd[j]; vals[5 * MM + j] = dBd[j];
-        vals[6 * MM + j] = dRn[j];
+        mix_stats_from_sums(dA[0][j], dA[1][j], dA[2][j], dA[3][j], dA[4][j], dA[5][j], dA[6][j],
+                            pr[j], a.grad_mode, a.update_rho, vals[kUs * MM + j], vals[kKn * MM + j],
+                            vals[kLn * MM + j], vals[kMn * MM + j], vals[kMd * MM + j],
+                            vals[kBd * MM + j], vals[kRn * MM + j]);
     }
     vals[7 * MM + 0] = dCn; vals[7 * MM + 1] = dS2; vals[7 * MM + 2] = dGs;
 #pragma unroll
