@@ -252,6 +252,67 @@ def reference_arm(args):
         shutil.rmtree(work, ignore_errors=True)
 
 
+def cohort_arm(args):
+    """Cohort workload: subjects with n in {32, 64, 128} (in turn), T uniform in
+    [100k, 800k] x scale, M = 1, m = 3, each from the single-model recipe with
+    seed 1000 + i and cond(A) uniform in [10, 50]; fitted concurrently (mixed
+    form, SMs split by the autotuner) against the same subjects fitted one after
+    another on the whole GPU with the plain form.  Host wall clock; every subject
+    runs warmup + steps iterations in both arms."""
+    import torch
+    from cudamica_b200 import synth
+    from cudamica_b200.cohort import Cohort
+    from cudamica_b200.engine import Amica
+    rng = np.random.default_rng(7)
+    S = args.cohort_subjects
+    data, inits = [], []
+    for i in range(S):
+        n = (32, 64, 128)[i % 3]
+        T = int(rng.uniform(100_000, 800_000) * args.cohort_scale)
+        cond = float(rng.uniform(10.0, 50.0))
+        d = synth.config1(seed=1000 + i, n=n, T=T, cond=cond)
+        data.append(d.x.astype(np.float32))
+        inits.append(synth.norand_init(n, 1))
+    nsm = torch.cuda.get_device_properties(0).multi_processor_count
+    coh = Cohort(data, M=1, m=3, precision=1, inits=inits, sm_budget=nsm, maxiter=4000)
+    coh.run(args.warmup)
+    outs, dt = coh.timed_run(args.steps)
+    cohort_ll = [o[-1].ll for o in outs]
+    grids = list(coh.grids)
+    coh.close()
+    seq_ms, seq_ll = 0.0, []
+    for x, init in zip(data, inits):
+        T, n = x.shape
+        eng = Amica(n, T, 1, 3, precision=0, maxiter=4000)
+        eng.load_data(x)
+        eng.preprocess()
+        eng.init(*init)
+        eng.run(args.warmup)
+        t0 = time.perf_counter()
+        o = eng.run(args.steps)
+        seq_ms += (time.perf_counter() - t0) * 1e3
+        seq_ll.append(o[-1].ll)
+        eng.close()
+    value = args.steps / dt
+    seq = 1000.0 * args.steps / seq_ms
+    d_ll = [abs(a - b) for a, b in zip(cohort_ll, seq_ll)]
+    return {
+        "metric": "cohort EM iters/s (all subjects one iteration each)", "value": value,
+        "unit": "cohort iters/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"cohort of {S} subjects, n in {{32,64,128}}, T ~ U[1e5, 8e5] x "
+                               f"{args.cohort_scale}, M=1, m=3",
+                   "subjects": S, "total_samples": int(sum(x.shape[0] for x in data)),
+                   "grids": grids, "parallelism": "single GPU, one stream per subject"},
+        "sequential_plain": {"value": seq, "ms_per_step": seq_ms / args.steps},
+        "speedup_vs_sequential_plain": value / seq,
+        "final_ll_abs_diff": {"max": max(d_ll), "median": float(np.median(d_ll)),
+                              "note": "per subject, cohort (mixed) vs sequential (plain), "
+                                      "after warmup + steps iterations"},
+    }
+
+
 def profile_case(args):
     """A few E-step launches per form on the first T samples of the workload."""
     from cudamica_b200.engine import Amica
@@ -282,9 +343,17 @@ def main():
                     help="no timing: run a few fused E-step launches of both forms on a "
                          "T-sample slice (for ncu captures)")
     ap.add_argument("--T", type=int, default=WORKLOAD["T"])
+    ap.add_argument("--cohort", action="store_true",
+                    help="the cohort workload instead of the single-fit one")
+    ap.add_argument("--cohort-subjects", type=int, default=48)
+    ap.add_argument("--cohort-scale", type=float, default=1.0,
+                    help="scale of the per-subject sample counts")
     args = ap.parse_args()
     if args.profile_case:
         return profile_case(args)
+    if args.cohort:
+        print(json.dumps(cohort_arm(args)))
+        return 0
     ws, rank, local = dist_env()
     pg = None
     if ws > 1:

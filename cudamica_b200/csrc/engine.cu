@@ -69,6 +69,7 @@ struct amica_ctx {
     int64_t T = 0;
     bool use_tc = false;
     int nclusters = 0, ntiles = 0, nslots = 0;   // nslots: partial-sum slots per model
+    int nclusters_cap = 0;                        // grid the partial-sum buffer was sized for
     bool have_data = false, have_x = false, have_init = false, have_estep = false;
 
     float* d_rawx = nullptr;     // T x n raw input (float)
@@ -92,6 +93,8 @@ struct amica_ctx {
     std::vector<IterRec> hist;    // host copy of the iteration history
 
     cudaGraphExec_t graph = nullptr;
+    int64_t pending = -1;         // iterations enqueued by amica_run_async, -1 if none
+    int64_t pending_it0 = 0;
 };
 
 namespace {
@@ -317,6 +320,10 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     c->ntiles = (int)((T + c->S - 1) / c->S);
     int maxcl = c->use_tc ? tc_max_clusters((int)n, (int)m, (int)M) : plain_max_clusters((int)n, (int)m, (int)M);
     if (maxcl <= 0) { amica_destroy(c); return AMICA_ERR_UNSUPPORTED; }
+    // partial-sum slots are sized for the full grid so that amica_set_grid can
+    // move between any grid sizes later
+    c->nclusters_cap = maxcl < c->ntiles ? maxcl : c->ntiles;
+    if (cfg->max_clusters > 0 && cfg->max_clusters < maxcl) maxcl = (int)cfg->max_clusters;
     c->nclusters = maxcl < c->ntiles ? maxcl : c->ntiles;
 
     MStepCfgHost& h = c->hc;
@@ -343,7 +350,7 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     AL(b.ltc64, M);
     PartLayout PL{(int)n, (int)m};
     c->nslots = c->nclusters * (c->use_tc ? tc_partial_groups() : 1);
-    AL(b.partial, (size_t)c->nslots * M * PL.stride());
+    AL(b.partial, (size_t)c->nclusters_cap * (c->use_tc ? tc_partial_groups() : 1) * M * PL.stride());
     AL(b.raw, M * (size_t)PL.stride());
     AL(b.stats, (size_t)amica_stats_len(n, M, m));
     AL(b.work, M * 4 * n);
@@ -546,13 +553,13 @@ int amica_em_step(amica_ctx* c, amica_iter_out* out) {
     return AMICA_OK;
 }
 
-int amica_run(amica_ctx* c, int64_t maxiter, amica_iter_out* hist) {
+int amica_run_async(amica_ctx* c, int64_t maxiter) {
     if (!c) return AMICA_ERR_INVALIDPARAM;
     if (!c->have_x || !c->have_init) return AMICA_ERR_STATE;
     if (maxiter < 0) return AMICA_ERR_INVALIDPARAM;
+    if (c->pending >= 0) return AMICA_ERR_STATE;      // a batch is still outstanding
     CK(cudaSetDevice(c->dev));
     if (!c->graph) {
-        // warm launch outside capture (sets kernel attributes), then capture
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
         int r = enqueue_iteration(c);
@@ -571,6 +578,17 @@ int amica_run(amica_ctx* c, int64_t maxiter, amica_iter_out* hist) {
     for (int64_t k = 0; k < maxiter; k++) CK(cudaGraphLaunch(c->graph, c->st));
     CK(cudaEventRecord(c->ev1, c->st));
     CK(cudaMemcpyAsync(c->h_ctrl, c->b.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    c->pending = maxiter;
+    c->pending_it0 = it0;
+    return AMICA_OK;
+}
+
+int amica_run_wait(amica_ctx* c, amica_iter_out* hist) {
+    if (!c) return AMICA_ERR_INVALIDPARAM;
+    if (c->pending < 0) return AMICA_ERR_STATE;
+    CK(cudaSetDevice(c->dev));
+    const int64_t maxiter = c->pending, it0 = c->pending_it0;
+    c->pending = -1;
     CK(cudaStreamSynchronize(c->st));
     c->have_estep = maxiter > 0 || c->have_estep;
     int e = check_device_error(c);
@@ -590,6 +608,32 @@ int amica_run(amica_ctx* c, int64_t maxiter, amica_iter_out* hist) {
         cudaStreamSynchronize(c->st);
     }
     return e;
+}
+
+int amica_set_grid(amica_ctx* c, int64_t max_clusters, int64_t* nclusters) {
+    if (!c || max_clusters < 0) return AMICA_ERR_INVALIDPARAM;
+    if (c->pending >= 0) return AMICA_ERR_STATE;
+    CK(cudaSetDevice(c->dev));
+    int maxcl = c->use_tc ? tc_max_clusters(c->n, c->m, c->M) : plain_max_clusters(c->n, c->m, c->M);
+    if (maxcl <= 0) return AMICA_ERR_UNSUPPORTED;
+    if (max_clusters > 0 && max_clusters < maxcl) maxcl = (int)max_clusters;
+    const int ncl = maxcl < c->ntiles ? maxcl : c->ntiles;
+    // the partial-sum slots were sized for the largest grid at creation
+    if (ncl > c->nclusters_cap) return AMICA_ERR_INVALIDPARAM;
+    c->nclusters = ncl;
+    c->nslots = ncl * (c->use_tc ? tc_partial_groups() : 1);
+    if (c->graph) {
+        CK(cudaStreamSynchronize(c->st));
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
+    if (nclusters) *nclusters = ncl;
+    return AMICA_OK;
+}
+
+int amica_run(amica_ctx* c, int64_t maxiter, amica_iter_out* hist) {
+    TRY(amica_run_async(c, maxiter));
+    return amica_run_wait(c, hist);
 }
 
 int amica_get_params(amica_ctx* c, double* A, double* W, double* cc, double* gm, double* alpha,

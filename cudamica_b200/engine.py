@@ -30,7 +30,7 @@ CFG_INT_FIELDS = (
     "nchannels", "nsamples", "nmmodels", "nsdm", "maxiter", "do_sphere", "block_size", "fix_init",
     "do_newton", "update_rho", "rho_start_iter", "newt_start_iter", "maxdec", "update_gm",
     "update_alpha", "update_A", "update_mu", "update_beta", "do_reparm", "do_reject", "rejstart",
-    "rejint", "maxrej", "precision", "device", "seed", "verbose")
+    "rejint", "maxrej", "precision", "device", "seed", "verbose", "max_clusters")
 CFG_DBL_FIELDS = ("lrate0", "lratemax", "lnatrate", "lratefact", "rho0", "rholrate", "rhomin",
                   "rhomax", "rejsig")
 
@@ -41,7 +41,8 @@ EXPORTED = (
     "amica_stats_len", "amica_get_loglik", "amica_loglik_adjoint", "amica_reject_now",
     "amica_write_outputs", "amica_status_string", "amica_kernel_name", "amica_get_p_relative",
     "amica_last_cuda_error", "amica_set_iter_state", "amica_get_sphere", "amica_time_estep",
-    "amica_launches_per_iteration", "amica_selftest_umma", "amica_estep_stats_noalloc")
+    "amica_launches_per_iteration", "amica_selftest_umma", "amica_estep_stats_noalloc",
+    "amica_run_async", "amica_run_wait", "amica_set_grid")
 
 
 class Cfg(C.Structure):
@@ -87,6 +88,9 @@ def lib():
         L.amica_init.argtypes = [vp, _pd, _pd]
         L.amica_em_step.argtypes = [vp, C.POINTER(IterOut)]
         L.amica_run.argtypes = [vp, _i64, C.POINTER(IterOut)]
+        L.amica_run_async.argtypes = [vp, _i64]
+        L.amica_set_grid.argtypes = [vp, _i64, C.POINTER(_i64)]
+        L.amica_run_wait.argtypes = [vp, C.POINTER(IterOut)]
         L.amica_get_params.argtypes = [vp] + [_pd] * 8
         L.amica_set_params.argtypes = [vp] + [_pd] * 7
         L.amica_estep_stats.argtypes = [vp, _pd]
@@ -225,6 +229,26 @@ class Amica:
     def run(self, iters: int) -> list:
         outs = (IterOut * max(iters, 1))()
         _chk(lib().amica_run(self._ctx, iters, outs), "amica_run")
+        return [outs[k] for k in range(iters)]
+
+    def set_grid(self, max_clusters: int) -> int:
+        """Cap the E-step grid at max_clusters clusters (0: all that fit); returns
+        the grid in effect."""
+        k = _i64()
+        _chk(lib().amica_set_grid(self._ctx, max_clusters, C.byref(k)), "amica_set_grid")
+        return int(k.value)
+
+    def run_async(self, iters: int) -> None:
+        """Enqueue `iters` iterations on this context's stream and return at once."""
+        _chk(lib().amica_run_async(self._ctx, iters), "amica_run_async")
+        self._pending = iters
+
+    def run_wait(self) -> list:
+        """Wait for the iterations of the last run_async and return their records."""
+        iters = getattr(self, "_pending", 0)
+        outs = (IterOut * max(iters, 1))()
+        _chk(lib().amica_run_wait(self._ctx, outs), "amica_run_wait")
+        self._pending = 0
         return [outs[k] for k in range(iters)]
 
     # -- state -------------------------------------------------------------

@@ -59,6 +59,8 @@ typedef struct amica_cfg {
     int64_t update_gm, update_alpha, update_A, update_mu, update_beta, do_reparm;
     int64_t do_reject, rejstart, rejint, maxrej;
     int64_t precision, device, seed, verbose;
+    int64_t max_clusters;   /* cap on the E-step grid in clusters (0: as many as fit); lets
+                               several contexts share the GPU's SMs concurrently (new key) */
     double lrate0, lratemax, lnatrate, lratefact, rho0, rholrate, rhomin, rhomax, rejsig;
 } amica_cfg;
 
@@ -210,6 +212,21 @@ int amica_estep_stats_noalloc(const float *x, int64_t ldx, int64_t n, int64_t T,
                               const double *mu, const double *beta, const double *rho,
                               const double *gm, double ldetS, const uint8_t *keep, int64_t nkeep,
                               int64_t update_rho, double *stats, void *stream);
+
+/* amica_run() in two halves, for driving several contexts (one per subject of
+ * a cohort, each on its own stream) concurrently: amica_run_async() enqueues
+ * `iters` replays of the iteration graph on the context's stream and returns
+ * at once; amica_run_wait() waits for them, fills hist[0..iters-1] when hist
+ * is not NULL, checks the device error flag and the LLs (rolling back to the
+ * parameters before the batch on NaN/Inf, as amica_run does).  No counterpart
+ * in the reference (its loop is synchronous). */
+int amica_run_async(amica_ctx *ctx, int64_t iters);
+/* Re-size the E-step grid of a created context to at most max_clusters clusters
+ * (0: as many as fit); *nclusters (may be NULL) receives the grid in effect.
+ * The iteration graph is re-captured on the next run.  No counterpart in the
+ * reference. */
+int amica_set_grid(amica_ctx *ctx, int64_t max_clusters, int64_t *nclusters);
+int amica_run_wait(amica_ctx *ctx, amica_iter_out *hist);
 
 /* Last CUDA runtime error code seen by any call (0 = none). */
 int amica_last_cuda_error(void);

@@ -1,0 +1,102 @@
+"""Cohort fitting: several contexts sharing the GPU concurrently.
+
+CPU: the SM split of autotune.split_budget.
+GPU: a cohort of subjects with different channel counts and lengths, run
+concurrently with capped grids, gives exactly (bit for bit) what each subject
+gives when fitted alone with the same grid -- the kernels are deterministic
+for a given grid and the subjects share nothing but the SMs.
+"""
+import numpy as np
+import pytest
+
+from cudamica_b200 import autotune, synth
+
+
+def test_split_budget_proportional_and_bounded():
+    work = [1.0, 2.0, 4.0, 1.0]
+    alloc = autotune.split_budget(work, 16)
+    assert sum(alloc) <= 16 and min(alloc) >= 1
+    assert alloc[2] >= alloc[1] >= alloc[0]
+    # clusters of M = 3 CTAs: SMs = 3 x clusters stay within the budget
+    alloc3 = autotune.split_budget([1.0, 1.0, 1.0], 20, [3, 3, 3])
+    assert sum(a * 3 for a in alloc3) <= 20 and min(alloc3) >= 1
+    # more subjects than SMs: everyone still gets one cluster
+    assert autotune.split_budget([1.0] * 5, 3) == [1, 1, 1, 1, 1]
+
+
+def subjects():
+    rng_specs = [(16, 12000, 1), (32, 20000, 2), (24, 9000, 3), (64, 30000, 4)]
+    data, inits = [], []
+    for n, T, seed in rng_specs:
+        d = synth.config1(seed=seed, n=n, T=T, outlier_frac=0.0)
+        data.append(d.x.astype(np.float32))
+        inits.append(synth.norand_init(n, 1))
+    return data, inits
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [1, 0])
+def test_cohort_matches_subjects_fitted_alone(precision):
+    from cudamica_b200.cohort import Cohort
+    from cudamica_b200.engine import Amica
+    data, inits = subjects()
+    # a split grid (the concurrency case that shares SMs); the tuned choice is
+    # exercised below
+    grids = autotune.split_budget([float(x.shape[0] * x.shape[1]) for x in data], 40)
+    coh = Cohort(data, M=1, m=3, precision=precision, inits=inits, grids=grids)
+    assert sum(coh.grids) <= 40
+    outs = coh.run(6)
+    for s, (x, init) in enumerate(zip(data, inits)):
+        T, n = x.shape
+        eng = Amica(n, T, 1, 3, precision=precision)
+        eng.load_data(x)
+        eng.preprocess()
+        eng.init(*init)
+        eng.set_grid(coh.grids[s])
+        alone = eng.run(6)
+        assert [o.ll for o in alone] == [o.ll for o in outs[s]], s
+        pa, pc = eng.params(), coh.engines[s].params()
+        for k in ("A", "mu", "beta", "rho", "alpha", "c"):
+            assert np.array_equal(pa[k], pc[k]), (s, k)
+        eng.close()
+    coh.close()
+
+
+@pytest.mark.gpu
+def test_grid_cap_keeps_results_close():
+    # a different grid changes only the summation order of the partial sums
+    from cudamica_b200.engine import Amica
+    data, inits = subjects()
+    x, init = data[3], inits[3]
+    T, n = x.shape
+    lls = []
+    for g in (0, 3):
+        eng = Amica(n, T, 1, 3, precision=0)
+        eng.load_data(x)
+        eng.preprocess()
+        eng.init(*init)
+        eng.set_grid(g)
+        lls.append(np.array([o.ll for o in eng.run(3)]))
+        eng.close()
+    assert np.max(np.abs(lls[0] - lls[1])) < 1e-6
+
+
+@pytest.mark.gpu
+def test_tuned_cohort_starts_from_the_initial_state():
+    from cudamica_b200.cohort import Cohort
+    from cudamica_b200.engine import Amica
+    data, inits = subjects()
+    coh = Cohort(data, M=1, m=3, precision=1, inits=inits)
+    assert set(coh.timings) >= {"whole_gpu", "split_1", "split_0.8"}
+    outs = coh.run(3)
+    for s, (x, init) in enumerate(zip(data, inits)):
+        assert [o.iter for o in outs[s]] == [1, 2, 3]
+        T, n = x.shape
+        eng = Amica(n, T, 1, 3, precision=1)
+        eng.load_data(x)
+        eng.preprocess()
+        eng.init(*init)
+        eng.set_grid(coh.grids[s])
+        assert [o.ll for o in eng.run(3)] == [o.ll for o in outs[s]]
+        eng.close()
+    coh.close()
