@@ -46,6 +46,23 @@ def dist_env():
     return ws, rank, local
 
 
+def reduce_over_ranks(values, pg, op: str, device: str = "cuda"):
+    """Element-wise max or min of `values` over all ranks (every rank calls it,
+    in the same order); identity without a process group."""
+    if pg is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX if op == "max" else pg.ReduceOp.MIN)
+    return [float(v) for v in t.cpu()]
+
+
+def whole_job_rate(ms_per_step_max: float, ws: int) -> float:
+    """Iterations per second of the whole job: every rank runs one iteration of
+    its own replica per step; the step takes as long as the slowest rank."""
+    return ws * 1000.0 / ms_per_step_max
+
+
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
@@ -412,12 +429,8 @@ def main():
     rng = np.random.default_rng(123)
     A0p = A0 * (1.0 + 1e-12 * rng.standard_normal(A0.shape))
     _, ll_ctrl, _, _, _ = time_form(x, A0p, c0, 0, device, 1, 0, args.fit_iters)
-    ms = t_mixed
-    if pg:
-        t = torch.tensor([ms, t_plain], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms, t_plain = float(t[0]), float(t[1])
-    value = ws * 1000.0 / ms
+    ms, t_plain = reduce_over_ranks([t_mixed, t_plain], pg, "max")
+    value = whole_job_rate(ms, ws)
     hbm, bf16, src = peaks()
     n, T, M, m = (WORKLOAD[k] for k in ("n", "T", "M", "m"))
     alg_bytes = 4 * n * T + 4 * M * T            # x read once + Lt write per iteration
@@ -442,7 +455,7 @@ def main():
                    "precision": "mixed: tcgen05 TF32 contractions, FP32 densities, FP64 M-step",
                    "kernel": kname, "l2": "inputs larger than L2 (512 MB sphered data per step)",
                    "parallelism": "replicas" if ws > 1 else "single GPU"},
-        "plain_fp32": {"value": ws * 1000.0 / t_plain, "ms_per_step": t_plain, "kernel": kname_plain,
+        "plain_fp32": {"value": whole_job_rate(t_plain, ws), "ms_per_step": t_plain, "kernel": kname_plain,
                        "estep_ms": est_plain},
         "mixed_over_plain": t_plain / ms,
         "final_ll": {"iters": args.fit_iters, "mixed": ll_mixed, "plain": ll_plain,
@@ -458,9 +471,7 @@ def main():
     if not args.no_e2e:
         e2e = e2e_run(x, A0, c0, device, args.steps)
         if pg:
-            t = torch.tensor([e2e["value"]], dtype=torch.float64, device="cuda")
-            pg.all_reduce(t, op=pg.ReduceOp.MIN)
-            e2e["value"] = float(t[0]) * ws
+            e2e["value"] = reduce_over_ranks([e2e["value"]], pg, "min")[0] * ws
         out["e2e"] = e2e
     if rank == 0:
         print(json.dumps(out))

@@ -233,3 +233,22 @@ def test_umma_layouts(mode, N, K):
     ref = Aref @ B.astype(np.float64).T
     err = np.max(np.abs(D - ref)) / np.max(np.abs(ref))
     assert err < (2e-6 if mode == 2 else 1e-6), (mode, N, K, err)
+
+
+def test_full_size_fit_is_repeatable():
+    # the n = 128, T = 1,000,000, M = 3 workload: the same inputs give the same
+    # LL trajectory bit for bit (fixed-order reductions throughout)
+    from cudamica_b200 import synth
+    from cudamica_b200.engine import Amica
+    d = synth.config2(seed=0, n=128, T=1_000_000, M=3, m=3)
+    A0, c0 = synth.norand_init(128, 3)
+    runs = []
+    for _ in range(2):
+        eng = Amica(128, 1_000_000, 3, 3, precision=1)
+        eng.load_data(d.x)
+        eng.preprocess()
+        eng.init(A0, c0)
+        runs.append([o.ll for o in eng.run(8)])
+        eng.close()
+    assert runs[0] == runs[1]
+    assert all(np.isfinite(runs[0]))

@@ -61,3 +61,27 @@ def test_scheduled_rejection_is_bit_exact():
         keep_prev = keep
     assert passes == 3
     eng.close()
+
+
+def test_rejection_bit_exact_at_full_size():
+    # the single-model EEG-scale workload: n = 64, T = 500,000, 0.5% of the
+    # samples in 20-sigma bursts, rejection every 10 iterations at 3 sigma
+    from cudamica_b200.engine import Amica
+    d = synth.config1(seed=0, n=64, T=500_000)
+    A0, c0 = synth.norand_init(64, 1)
+    for precision in (1, 0):
+        eng = Amica(64, 500_000, 1, 3, precision=precision, do_reject=1, rejstart=10, rejint=10,
+                    maxrej=3, rejsig=3.0)
+        eng.load_data(d.x.astype(np.float32))
+        eng.preprocess()
+        eng.init(A0, c0)
+        eng.run(9)
+        keep_prev = eng.loglik()[2].copy()
+        out = eng.step()                                  # iteration 10: a rejection pass
+        P = eng.p_relative().astype(np.float64)
+        keep = eng.loglik()[2]
+        k_o, d_o, _, _ = O.reject(P, keep_prev, 3.0)
+        assert np.array_equal(keep, k_o)
+        assert out.nrejected == d_o > 0
+        assert (keep == 0)[d.outliers].mean() > 0.95
+        eng.close()
