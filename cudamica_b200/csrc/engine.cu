@@ -31,8 +31,9 @@ cudaError_t launch_estep_plain(const EStepArgs& a, int NP, int nclusters, cudaSt
 // estep_tc.cu
 int tc_supported(int n, int m, int M);
 int tc_max_clusters(int n, int m, int M);
-int tc_tile_samples();
-int tc_partial_groups();
+int tc_tile_samples(int n);
+int tc_partial_groups(int n);
+int tc_psi_step();
 int tc_selftest(int mode, int N, int K, const float* hA, const float* hB, float* hD, int* derr);
 cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStream_t st);
 // preprocess.cu
@@ -316,7 +317,7 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     CK(cudaEventCreate(&c->ev1));
 
     c->use_tc = (cfg->precision == AMICA_PREC_MIXED) && tc_supported((int)n, (int)m, (int)M);
-    c->S = c->use_tc ? tc_tile_samples() : plain_tile_samples();
+    c->S = c->use_tc ? tc_tile_samples((int)n) : plain_tile_samples();
     c->ntiles = (int)((T + c->S - 1) / c->S);
     int maxcl = c->use_tc ? tc_max_clusters((int)n, (int)m, (int)M) : plain_max_clusters((int)n, (int)m, (int)M);
     if (maxcl <= 0) { amica_destroy(c); return AMICA_ERR_UNSUPPORTED; }
@@ -339,7 +340,7 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     h.rholrate = cfg->rholrate; h.rhomin = cfg->rhomin; h.rhomax = cfg->rhomax;
     h.rejsig = cfg->rejsig; h.ldetS = 0.0;
     h.psi_is_phi = c->use_tc ? 1 : 0;
-    h.psi_step = c->use_tc ? tc_partial_groups() : 1;
+    h.psi_step = c->use_tc ? tc_psi_step() : 1;
 
     MStepBuffers& b = c->b;
     const size_t nn = (size_t)n * n, mn = (size_t)m * n;
@@ -349,8 +350,9 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     AL(b.beta, M * mn); AL(b.rho, M * mn); AL(b.gm, M); AL(b.W, M * nn); AL(b.ldet, M);
     AL(b.ltc64, M);
     PartLayout PL{(int)n, (int)m};
-    c->nslots = c->nclusters * (c->use_tc ? tc_partial_groups() : 1);
-    AL(b.partial, (size_t)c->nclusters_cap * (c->use_tc ? tc_partial_groups() : 1) * M * PL.stride());
+    const int groups = c->use_tc ? tc_partial_groups((int)n) : 1;
+    c->nslots = c->nclusters * groups;
+    AL(b.partial, (size_t)c->nclusters_cap * groups * M * PL.stride());
     AL(b.raw, M * (size_t)PL.stride());
     AL(b.stats, (size_t)amica_stats_len(n, M, m));
     AL(b.work, M * 4 * n);
@@ -364,7 +366,9 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     AL(b.hist, b.hist_cap);
     AL(b.err, 1);
     AL(c->d_keep, T); AL(c->d_Lt, M * T); AL(c->d_P, T);
-    AL(c->d_x, (size_t)T * NP);
+    // 3 zero samples past T: the tensor-core form reads the data as rows of up
+    // to 4 samples
+    AL(c->d_x, (size_t)(T + 3) * NP);
     AL(c->d_means, n); AL(c->d_sphere, nn); AL(c->d_cov, nn); AL(c->d_evwork, 4 * nn + 4 * n);
     AL(c->d_ldetS, 1);
     c->backup_len = param_len(c) + (sizeof(Ctrl) + 7) / 8;
@@ -621,7 +625,7 @@ int amica_set_grid(amica_ctx* c, int64_t max_clusters, int64_t* nclusters) {
     // the partial-sum slots were sized for the largest grid at creation
     if (ncl > c->nclusters_cap) return AMICA_ERR_INVALIDPARAM;
     c->nclusters = ncl;
-    c->nslots = ncl * (c->use_tc ? tc_partial_groups() : 1);
+    c->nslots = ncl * (c->use_tc ? tc_partial_groups(c->n) : 1);
     if (c->graph) {
         CK(cudaStreamSynchronize(c->st));
         cudaGraphExecDestroy(c->graph);

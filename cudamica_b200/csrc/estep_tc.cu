@@ -1,21 +1,23 @@
 // Mixed-precision fused AMICA E-step on the 5th-generation tensor cores
 // (tcgen05, TF32 operands, FP32 accumulation in tensor memory).
 //
-// Cluster of M CTAs, CTA rank h = model h; persistent over 64-sample tiles.
-//   warp 16 (control): TMA loads of the x tile (128B-swizzled, two stages),
+// Cluster of M CTAs, CTA rank h = model h; persistent over tiles of 48 rows of
+// the data (a row is one sample, or R samples side by side when n <= 64: see
+// "Lane packing" below).
+//   warp 12 (control): TMA loads of the x tile (128B-swizzled, two stages),
 //     and the two contractions issued by one thread:
-//       MMA1  b_h = W_hi x^T + W_lo x^T   M=128 (channels) N=48 (samples) K=n
+//       MMA1  b_h = W_hi x^T + W_lo x^T   M=128 (lanes) N=48 (rows) K=128
 //             W_hi = tf32(W_h) K-major in smem, W_lo = tf32(W_h - W_hi) in TMEM,
 //             B = x tile (K-major, TMA), D -> TMEM (2 buffers)
-//       MMA2  phi_h += G B^T            M=128 N=n K=48
+//       MMA2  phi_h += G B^T            M=128 N=128 K=48
 //             A = G, B = the b tile, both K-major tiles written by the density
 //             warps, D -> TMEM for the CTA's life
-//   warps 0-15 (4 warpgroups x 4 warps): thread = (channel = TMEM lane,
-//     warpgroup = 16-sample slice).  Each reads its b values with tcgen05.ld,
-//     evaluates the generalized-Gaussian mixture densities and the log-sum-exp
-//     over mixtures (FP32, MUFU ex2/lg2), reduces over channels with warp
-//     shuffles, exchanges the per-sample Lt_h(t) with the other models' CTAs
-//     through distributed shared memory + remote mbarrier arrivals, forms
+//   warps 0-11 (3 warpgroups x 4 warps): thread = (TMEM lane, warpgroup =
+//     16-row slice).  Each reads its b values with tcgen05.ld, evaluates the
+//     generalized-Gaussian mixture densities and the log-sum-exp over
+//     mixtures (FP32, MUFU ex2/lg2), reduces over channels with warp shuffles,
+//     exchanges the per-sample Lt_h(t) with the other models' CTAs through
+//     distributed shared memory (st.async onto the peers' mbarriers), forms
 //     P(t) and v_h(t), accumulates the sufficient statistics and writes
 //     g = sum_j sqrt(beta) u f' and b = W (x - c) into the MMA2 operand tiles.
 // (An MN-major TF32 operand needs the 32-byte-atom 128B swizzle, which the
@@ -102,17 +104,11 @@ __device__ __forceinline__ uint32_t mapa(uint32_t addr, uint32_t rank) {
     asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
     return r;
 }
-__device__ __forceinline__ void st_cluster_f32(uint32_t addr, float v) {
-    asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(addr), "f"(v) : "memory");
-}
 // Asynchronous 4-byte store into a cluster peer's shared memory; completion is
 // counted on that peer's mbarrier as transaction bytes (no fence needed).
 __device__ __forceinline__ void st_async_f32(uint32_t addr, float v, uint32_t bar) {
     asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f32 [%0], %1, [%2];"
                  ::"r"(addr), "f"(v), "r"(bar) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_remote(uint32_t addr) {
-    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(addr) : "memory");
 }
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
                                             uint64_t* bar) {
@@ -179,14 +175,6 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
                  :: "memory");
 #pragma unroll
     for (int q = 0; q < 16; q++) v[q] = __uint_as_float(r[q]);
-}
-__device__ __forceinline__ void tmem_ld4(uint32_t taddr, float* v) {
-    uint32_t r0, r1, r2, r3;
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
-                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r0), "+r"(r1), "+r"(r2), "+r"(r3) :: "memory");
-    v[0] = __uint_as_float(r0); v[1] = __uint_as_float(r1);
-    v[2] = __uint_as_float(r2); v[3] = __uint_as_float(r3);
 }
 __device__ __forceinline__ void tmem_st4_nowait(uint32_t taddr, const float* v) {
     asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};"
@@ -277,12 +265,20 @@ enum { BAR_FULL0 = 0, BAR_FULL1, BAR_EMPTY0, BAR_EMPTY1, BAR_BFULL0, BAR_BFULL1,
        BAR_BEMPTY1, BAR_GFULL, BAR_GEMPTY, BAR_PSI, BAR_DRAIN,
        BAR_LT0 /* 2 parities x kWG warpgroups: BAR_LT0 + par * kWG + wg */ };
 
+// Lane packing: with npc (n padded to 32, 64 or 128) channels, the 128 TMEM
+// lanes hold R = 128 / npc sample sets side by side.  The sphered data
+// (T x npc floats, sample-major) is read as a (T / R) x 128 matrix whose row p
+// holds samples pR .. pR + R - 1; W_h enters as the block-diagonal
+// diag(W_h, ..., W_h), so lane r*npc + i of MMA1 yields b_i of sample pR + r.
+// Lanes of set r sum over their own channels; the statistics of set r go to
+// their own partial slots (folded with every other slot by the fixed-order
+// reduction), and phi_h is the sum of the R diagonal blocks of g b^T.
 struct TcArgs {
     EStepArgs e;
-    int ngroups;   // partial slots per cluster (one per warpgroup)
+    int ngroups;   // partial slots per cluster: kWG per sample set, set-major
 };
 
-template <int NP, int MM>
+template <int NP, int MM, int R>
 __global__ void __launch_bounds__(kThreads, 1)
     estep_tc_kernel(const __grid_constant__ CUtensorMap xmap, TcArgs ta) {
     using Sh = TcShape<NP>;
@@ -324,11 +320,16 @@ __global__ void __launch_bounds__(kThreads, 1)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     {
-        const float* Wh = a.Wf + (size_t)h * NP * NP;   // W[i][k], rows i >= NP are zero
+        // block-diagonal diag(W_h, ..., W_h) of R blocks of npc x npc; W[i][k]
+        // row-major with stride npc, rows i >= n zero
+        constexpr int npc = NP / R;
+        const float* Wh = a.Wf + (size_t)h * npc * npc;
         for (int e4 = tid; e4 < 128 * (NP / 4); e4 += kThreads) {
             const int i = e4 / (NP / 4), k = (e4 % (NP / 4)) * 4;
+            const int si = i / npc, sk = k / npc;
             float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (i < NP) v = *reinterpret_cast<const float4*>(Wh + (size_t)i * NP + k);
+            if (si == sk)
+                v = *reinterpret_cast<const float4*>(Wh + (size_t)(i - si * npc) * npc + (k - sk * npc));
             v.x = tf32_rna(v.x); v.y = tf32_rna(v.y); v.z = tf32_rna(v.z); v.w = tf32_rna(v.w);
             *reinterpret_cast<float4*>((uint8_t*)Wsm + sw128_off(i, k, 128)) = v;
         }
@@ -348,13 +349,16 @@ __global__ void __launch_bounds__(kThreads, 1)
     // second half of MMA1, so that b = W_hi x + W_lo x keeps W to ~2^-22
     if (warp < 4) {
         const int i = warp * 32 + lane;
-        const float* Wrow = a.Wf + ((size_t)h * NP + (i < NP ? i : 0)) * NP;
+        constexpr int npc = NP / R;
+        const int si = i / npc;
+        const float* Wrow = a.Wf + ((size_t)h * npc + (i - si * npc)) * npc;
 #pragma unroll 1
         for (int k0 = 0; k0 < NP; k0 += 16) {
             float lo[16];
+            const bool blk = (k0 / npc) == si;   // 16 columns never straddle a block
 #pragma unroll
             for (int q = 0; q < 16; q++) {
-                const float w = (i < NP) ? Wrow[k0 + q] : 0.f;
+                const float w = blk ? Wrow[k0 - si * npc + q] : 0.f;
                 lo[q] = tf32_rna(w - tf32_rna(w));
             }
             tmem_st16(tmem + kWloCol + ((uint32_t)(warp * 32) << 16) + (uint32_t)k0, lo);
@@ -433,7 +437,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             // MMA2 for the last tile
             if (ok) {
-                const int kp = ntile_local - 1, sp = kp & 1;
+                const int kp = ntile_local - 1;
                 ok = mbar_wait(&bar[BAR_GFULL], (uint32_t)(kp & 1), abort_flag, a.err);
                 if (ok) {
                     tc_fence_after();
@@ -458,7 +462,12 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else {
         // =========================== density warps =================================
         const int wg = warp >> 2, q4 = warp & 3;
-        const int ch = q4 * 32 + lane;             // channel = TMEM lane
+        constexpr int npc = NP / R;
+        constexpr int wps = npc / 32;              // warps per sample set
+        const int set = q4 / wps;                  // this warp's sample set
+        const bool lead = (q4 % wps) == 0;         // first warp of its set
+        const int tl = q4 * 32 + lane;             // TMEM lane = row of the G / b tiles
+        const int ch = tl - set * npc;             // channel of this lane
         const bool ch_ok = ch < n;
         const uint32_t lane_addr = (uint32_t)(q4 * 32) << 16;
         // log2|y| of phase 1 is kept in tensor memory for phase 2 when it fits
@@ -472,9 +481,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         MixV<float> P1;
 #pragma unroll
         for (int j = 0; j < MM; j++) {
-            const MixParam q = a.mp[((size_t)h * MM + j) * NP + (ch < NP ? ch : 0)];
-            const float sj = ch < NP ? q.s : 0.f, oj = ch < NP ? -q.off : 0.f;
-            const float cj = ch < NP ? q.cl2 : 0.f, rj = ch < NP ? q.rho : 1.f;
+            const MixParam q = a.mp[((size_t)h * MM + j) * npc + ch];
+            const float sj = q.s, oj = -q.off;
+            const float cj = q.cl2, rj = q.rho;
             pr[j] = rj;
             if (j < 2 * NPR) {
                 float2* f[5] = {&P2[j / 2].s, &P2[j / 2].npo, &P2[j / 2].pc, &P2[j / 2].pr, &P2[j / 2].sr};
@@ -488,11 +497,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                 P1.s = sj; P1.npo = oj; P1.pc = cj; P1.pr = rj; P1.sr = sj * rj;
             }
         }
-        const float wci = ch < NP ? a.wc[(size_t)h * NP + ch] : 0.f;
+        const float wci = a.wc[(size_t)h * npc + ch];
         float ltc_all[kMaxModels];
 #pragma unroll
         for (int q = 0; q < kMaxModels; q++) ltc_all[q] = (q < M) ? (float)(a.ltc64[q] - a.ltc64[0]) : 0.f;
-        float* lse_sm = (float*)(sm + Sh::OFF_LSE) + (size_t)wg * kSub * 128 + ch;
+        float* lse_sm = (float*)(sm + Sh::OFF_LSE) + (size_t)wg * kSub * 128 + tl;
 
         // Per (channel, mixture), with u = v z, p = |y|^rho, r = 1/y:
         //   A0 = sum u, A1 = sum u p, A2 = sum u p^2, A3 = sum u p log2|y|,
@@ -521,10 +530,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         };
         zero_acc();
         double dLL = 0.0, dVs = 0.0;
-        // this thread's partial slot (one per warpgroup)
+        // this thread's partial slot (one per warpgroup and sample set)
         PartLayout L{n, MM};
-        double* out = a.partial + ((size_t)(cid * ta.ngroups + wg) * M + h) * L.stride();
-        double* out0 = a.partial + ((size_t)(cid * ta.ngroups) * M + h) * L.stride();  // phi lives here
+        double* out = a.partial + ((size_t)(cid * ta.ngroups + set * kWG + wg) * M + h) * L.stride();
+        // phi of this set lives in its warpgroup-0 slot
+        double* out0 = a.partial + ((size_t)(cid * ta.ngroups + set * kWG) * M + h) * L.stride();
         auto flush = [&]() {
             if (ch_ok) {
 #pragma unroll
@@ -559,9 +569,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int k = 0; k < ntile_local && ok; k++) {
             const int s = k & 1;
             const uint32_t u = (uint32_t)(k >> 1);
+            // packed rows of this warpgroup's slice; lane t < kSub owns row t0 + t,
+            // i.e. sample (t0 + t) R + set
             const int64_t t0 = ((int64_t)cid + (int64_t)k * a.nclusters) * kS + wg * kSub;
             // this tile's keep flags, fetched now and used after the exchange
-            const int64_t tk = t0 + (lane < kSub ? lane : kSub - 1);
+            const int64_t tk = (t0 + (lane < kSub ? lane : kSub - 1)) * R + set;
             const bool in_range = tk < a.T;
             const bool kept = in_range && (a.keep == nullptr || a.keep[tk]);
             const int par = k & 1;
@@ -645,7 +657,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                 for (int q = 0; q < kMaxModels; q++) {
                     if (q < M) {
                         const float* sq = slot + (par * kMaxModels + q) * 4 * kS + wg * kSub + t;
-                        Lq[q] = ltc_all[q] + kLn2 * (((sq[0] + sq[kS]) + sq[2 * kS]) + sq[3 * kS]);
+                        // this set's warps, in order
+                        float sw = sq[set * wps * kS];
+#pragma unroll
+                        for (int w = 1; w < wps; w++) sw += sq[(set * wps + w) * kS];
+                        Lq[q] = ltc_all[q] + kLn2 * sw;
                         lmax = fmaxf(lmax, Lq[q]);
                     }
                 }
@@ -662,7 +678,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const int64_t tg = tk;
                 const bool valid = kept;
                 vme = valid ? vh : 0.f;
-                if (q4 == 0 && lane < kSub) {
+                if (lead && lane < kSub) {
                     if (valid) {
                         dVs += (double)vh;
                         if (h == 0) dLL += (double)P;
@@ -726,7 +742,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     gq[r] = tf32_rna(g);
                     bq[r] = ch_ok ? tf32_rna(bb) : 0.f;
                 }
-                const uint32_t goff = sw128_off(ch, wg * kSub + g4 * 4, 128);
+                const uint32_t goff = sw128_off(tl, wg * kSub + g4 * 4, 128);
                 *reinterpret_cast<float4*>((uint8_t*)Gsm + goff) = make_float4(gq[0], gq[1], gq[2], gq[3]);
                 *reinterpret_cast<float4*>(sm + Sh::OFF_BT + goff) = make_float4(bq[0], bq[1], bq[2], bq[3]);
             }
@@ -740,8 +756,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             if ((k + 1) % kFlush == 0) flush();
         }
         flush();
-        // vsum / LL of this warpgroup (warp q4 == 0 accumulated them)
-        if (q4 == 0) {
+        // vsum / LL of this warpgroup and set (its first warp accumulated them)
+        if (lead) {
             double a1 = dLL, a2 = dVs;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -753,16 +769,17 @@ __global__ void __launch_bounds__(kThreads, 1)
                 out[1] = a2;
             }
         }
-        // ---- Psi_h out of tensor memory: warpgroup wg reads columns [wg*NP/4, (wg+1)*NP/4)
+        // ---- Psi_h out of tensor memory: the diagonal block of this set (columns
+        // [set*npc, set*npc + npc)), in 16-column chunks dealt round-robin to the
+        // warpgroups; the R blocks are summed by the slot reduction
         if (ok && ntile_local > 0) ok = mbar_wait(&bar[BAR_PSI], 0u, abort_flag, a.err);
         if (ok && ntile_local > 0) {
             tc_fence_after();
-            // 16-column chunks of Psi, dealt round-robin to the warpgroups
 #pragma unroll
-            for (int c0 = 0; c0 < NP; c0 += 16) {
+            for (int c0 = 0; c0 < npc; c0 += 16) {
                 if ((c0 / 16) % kWG != wg) continue;
                 float v[16];
-                tmem_ld16(tmem_psi + lane_addr + (uint32_t)c0, v);
+                tmem_ld16(tmem_psi + lane_addr + (uint32_t)(set * npc + c0), v);
 #pragma unroll
                 for (int q = 0; q < 16; q++) {
                     const int kcol = c0 + q;
@@ -889,14 +906,23 @@ PFN_encodeTiled get_encode() {
     return fn;
 }
 
-template <int NP, int MM>
+// Channels per packed sample set and sets per 128 lanes.
+int tc_np(int n) { return n <= 32 ? 32 : (n <= 64 ? 64 : 128); }
+int tc_pack(int n) { return 128 / tc_np(n); }
+
+// a.x holds at least ceil(T / R) * R samples of a.ldx = npc floats (samples at
+// and beyond T zero); it is read as ceil(T / R) rows of 128 floats.
+template <int NP, int MM, int R>
 cudaError_t launch_tc(const EStepArgs& a, int nclusters, cudaStream_t st) {
     using Sh = TcShape<NP>;
     PFN_encodeTiled enc = get_encode();
     if (!enc) return cudaErrorNotSupported;
+    if (a.ldx * R != NP) return cudaErrorInvalidValue;
+    const int64_t rows = (a.T + R - 1) / R;
+    if (a.ntiles != (int)((rows + kS - 1) / kS)) return cudaErrorInvalidValue;
     CUtensorMap map;
-    cuuint64_t dims[2] = {(cuuint64_t)a.ldx, (cuuint64_t)a.T};
-    cuuint64_t strides[1] = {(cuuint64_t)a.ldx * 4};
+    cuuint64_t dims[2] = {(cuuint64_t)NP, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)NP * 4};
     cuuint32_t box[2] = {32, (cuuint32_t)kS};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)a.x, dims, strides, box, estr,
@@ -904,12 +930,12 @@ cudaError_t launch_tc(const EStepArgs& a, int nclusters, cudaStream_t st) {
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
     const size_t smem = Sh::BYTES + 1024;
-    auto kern = estep_tc_kernel<NP, MM>;
+    auto kern = estep_tc_kernel<NP, MM, R>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     TcArgs ta;
     ta.e = a;
-    ta.ngroups = kWG;
+    ta.ngroups = kWG * R;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(nclusters * a.M);
     cfg.blockDim = dim3(kThreads);
@@ -925,11 +951,11 @@ cudaError_t launch_tc(const EStepArgs& a, int nclusters, cudaStream_t st) {
     return cudaLaunchKernelEx(&cfg, kern, map, ta);
 }
 
-template <int NP, int MM>
+template <int NP, int MM, int R>
 int tc_active_clusters(int M) {
     using Sh = TcShape<NP>;
     const size_t smem = Sh::BYTES + 1024;
-    auto kern = estep_tc_kernel<NP, MM>;
+    auto kern = estep_tc_kernel<NP, MM, R>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return -1;
     cudaLaunchConfig_t cfg = {};
@@ -979,42 +1005,37 @@ int tc_selftest(int mode, int N, int K, const float* hA, const float* hB, float*
     return e == cudaSuccess ? 0 : -20;
 }
 
-int tc_tile_samples() { return kS; }
-int tc_partial_groups() { return kWG; }
+// Samples per tile: kS packed rows of R samples each.
+int tc_tile_samples(int n) { return kS * tc_pack(n); }
+// Partial slots per cluster, and the stride between the slots that carry phi.
+int tc_partial_groups(int n) { return kWG * tc_pack(n); }
+int tc_psi_step() { return kWG; }
 
 int tc_supported(int n, int m, int M) {
     return n >= 2 && n <= 128 && m >= 1 && m <= 5 && M >= 1 && M <= kMaxModels;
 }
 
-static int tc_np(int n) { return n <= 32 ? 32 : (n <= 64 ? 64 : 128); }
-
+// Every channel count runs the 128-lane kernel (packed below 65 channels).
 int tc_max_clusters(int n, int m, int M) {
     if (!tc_supported(n, m, M)) return -1;
-    const int NP = tc_np(n);
-#define AMICA_TC_OCC(NPV, MMV) \
-    if (NP == NPV && m == MMV) return tc_active_clusters<NPV, MMV>(M);
-#define AMICA_TC_OCC_NP(NPV) \
-    AMICA_TC_OCC(NPV, 1) AMICA_TC_OCC(NPV, 2) AMICA_TC_OCC(NPV, 3) AMICA_TC_OCC(NPV, 4) \
-    AMICA_TC_OCC(NPV, 5)
-    AMICA_TC_OCC_NP(32)
-    AMICA_TC_OCC_NP(64)
-    AMICA_TC_OCC_NP(128)
-#undef AMICA_TC_OCC_NP
+    const int R = tc_pack(n);
+#define AMICA_TC_OCC(MMV) \
+    if (m == MMV) return R == 1 ? tc_active_clusters<128, MMV, 1>(M) \
+                                : (R == 2 ? tc_active_clusters<128, MMV, 2>(M) \
+                                          : tc_active_clusters<128, MMV, 4>(M));
+    AMICA_TC_OCC(1) AMICA_TC_OCC(2) AMICA_TC_OCC(3) AMICA_TC_OCC(4) AMICA_TC_OCC(5)
 #undef AMICA_TC_OCC
     return -1;
 }
 
 cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStream_t st) {
-    if (NP != tc_np(a.n)) return cudaErrorInvalidValue;
-#define AMICA_TC_CASE(NPV, MMV) \
-    if (NP == NPV && a.m == MMV) return launch_tc<NPV, MMV>(a, nclusters, st);
-#define AMICA_TC_NP(NPV) \
-    AMICA_TC_CASE(NPV, 1) AMICA_TC_CASE(NPV, 2) AMICA_TC_CASE(NPV, 3) AMICA_TC_CASE(NPV, 4) \
-    AMICA_TC_CASE(NPV, 5)
-    AMICA_TC_NP(32)
-    AMICA_TC_NP(64)
-    AMICA_TC_NP(128)
-#undef AMICA_TC_NP
+    if (NP != tc_np(a.n) || a.ldx != NP) return cudaErrorInvalidValue;
+    const int R = tc_pack(a.n);
+#define AMICA_TC_CASE(MMV) \
+    if (a.m == MMV) return R == 1 ? launch_tc<128, MMV, 1>(a, nclusters, st) \
+                                  : (R == 2 ? launch_tc<128, MMV, 2>(a, nclusters, st) \
+                                            : launch_tc<128, MMV, 4>(a, nclusters, st));
+    AMICA_TC_CASE(1) AMICA_TC_CASE(2) AMICA_TC_CASE(3) AMICA_TC_CASE(4) AMICA_TC_CASE(5)
 #undef AMICA_TC_CASE
     return cudaErrorInvalidValue;
 }
