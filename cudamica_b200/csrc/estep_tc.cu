@@ -4,7 +4,9 @@
 // Cluster of M CTAs, CTA rank h = model h; persistent over tiles of 48 rows of
 // the data (a row is one sample, or R samples side by side when n <= 64: see
 // "Lane packing" below).
-//   warp 12 (control): TMA loads of the x tile (128B-swizzled, two stages),
+//   warp 12 (control; warps 13-15 of its warpgroup idle, so that setmaxnreg
+//     can move registers to the density warpgroups): TMA loads of the x tile
+//     (128B-swizzled, two stages),
 //     and the two contractions issued by one thread:
 //       MMA1  b_h = W_hi x^T + W_lo x^T   M=128 (lanes) N=48 (rows) K=128
 //             W_hi = tf32(W_h) K-major in smem, W_lo = tf32(W_h - W_hi) in TMEM,
@@ -41,9 +43,17 @@ using namespace amica;
 namespace {
 
 constexpr int kS = 48;                  // samples per tile (MMA1 N)
-constexpr int kWG = 3;                  // density warpgroups (13 warps: <= 128 registers)
+constexpr int kWG = 3;                  // density warpgroups
 constexpr int kDensWarps = 4 * kWG;     // 12
-constexpr int kThreads = (kDensWarps + 1) * 32;
+constexpr int kThreads = (kDensWarps + 4) * 32;   // + one control warpgroup
+// Register split (setmaxnreg, per warpgroup): launched at 128 per thread
+// (512 x 128 = 65536), the control warpgroup drops to 96 (its unrolled MMA
+// issue needs about 80) and the three density warpgroups rise to 136:
+// 3 x 128 x 136 + 128 x 96 = 64512.  Measured at n=128, T=1M, M=3, m=3:
+// 136 beats 128 (no split, 3.37 ms), 144, 152 and 160 (3.18 against 3.24-3.41 ms).
+constexpr int kCtlRegs = 96;
+constexpr int kDensRegs = 136;
+static_assert(3 * 128 * kDensRegs + 128 * kCtlRegs <= kThreads * 128, "register split");
 constexpr int kSub = kS / kWG;          // 16 samples per thread per tile
 constexpr int kBcol = 64;               // TMEM column stride of the two b buffers
 constexpr int kPsiCol = 128;            // TMEM column of phi (N = NP columns)
@@ -368,9 +378,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     tc_fence_after();
 
-    if (warp == kDensWarps) {
-        // =========================== control warp: TMA + MMA =====================
-        if (lane == 0 && ntile_local > 0) {
+    if (warp >= kDensWarps) {
+        // =========================== control warpgroup: TMA + MMA ================
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kCtlRegs));
+        if (warp == kDensWarps && lane == 0 && ntile_local > 0) {
             const uint32_t x_off[2] = {Sh::OFF_X0, Sh::OFF_X1};
             const uint32_t sbase = smem_u32(sm);
             auto issue_tma = [&](int k) {
@@ -461,6 +472,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         __syncwarp();
     } else {
         // =========================== density warps =================================
+        asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kDensRegs));
         const int wg = warp >> 2, q4 = warp & 3;
         constexpr int npc = NP / R;
         constexpr int wps = npc / 32;              // warps per sample set
