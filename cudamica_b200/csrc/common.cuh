@@ -97,6 +97,7 @@ struct EStepArgs {
 struct MStepBuffers {
     double *A, *Anew, *c, *alpha, *mu, *beta, *rho, *gm, *W, *ldet, *ltc64;
     double *partial, *raw, *stats, *work, *chunk;
+    double* gj;        // n > 128: M n^2 working matrices + M n pivot logs of the inverse
     int64_t* bflag;
     int* use_newton;
     float *Wf, *wcf;

@@ -25,6 +25,7 @@
 namespace amica {
 // estep_plain.cu
 int plain_pad_channels(int n);
+int plain_partial_groups(int n);
 int plain_max_clusters(int n, int m, int M);
 int plain_tile_samples();
 cudaError_t launch_estep_plain(const EStepArgs& a, int NP, int nclusters, cudaStream_t st);
@@ -39,7 +40,7 @@ cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStrea
 // preprocess.cu
 cudaError_t launch_preprocess(const float* raw, int64_t T, int n, int do_sphere, double* means,
                               double* cov, double* sphere, double* evwork, double* ldetS_dev,
-                              float* x, int ldx, int tf32, cudaStream_t st);
+                              float* x, int ldx, int tf32, int* err, cudaStream_t st);
 cudaError_t launch_convert_sphered(const double* xs, int64_t T, int n, float* x, int ldx, int tf32,
                                    cudaStream_t st);
 // adjoint.cu
@@ -350,7 +351,7 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     AL(b.beta, M * mn); AL(b.rho, M * mn); AL(b.gm, M); AL(b.W, M * nn); AL(b.ldet, M);
     AL(b.ltc64, M);
     PartLayout PL{(int)n, (int)m};
-    const int groups = c->use_tc ? tc_partial_groups((int)n) : 1;
+    const int groups = c->use_tc ? tc_partial_groups((int)n) : plain_partial_groups((int)n);
     c->nslots = c->nclusters * groups;
     AL(b.partial, (size_t)c->nclusters_cap * groups * M * PL.stride());
     AL(b.raw, M * (size_t)PL.stride());
@@ -358,6 +359,7 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     AL(b.work, M * 4 * n);
     const int64_t nch = (T + 4095) / 4096;
     AL(b.chunk, 2 * nch + 2);
+    if (n > 128) AL(b.gj, (size_t)M * nn + (size_t)M * n);
     AL(b.bflag, M); AL(b.use_newton, M);
     AL(b.Wf, (size_t)M * NP * NP); AL(b.wcf, (size_t)M * NP); AL(b.mp, (size_t)M * m * NP);
     AL(b.ctrl, 1);
@@ -389,7 +391,7 @@ int amica_destroy(amica_ctx* c) {
     if (c->graph) cudaGraphExecDestroy(c->graph);
     void* ptrs[] = {c->b.A, c->b.Anew, c->b.c, c->b.alpha, c->b.mu, c->b.beta, c->b.rho, c->b.gm,
                     c->b.W, c->b.ldet, c->b.ltc64, c->b.partial, c->b.raw, c->b.stats,
-                    c->b.work, c->b.chunk, c->b.bflag, c->b.use_newton, c->b.Wf, c->b.wcf,
+                    c->b.work, c->b.chunk, c->b.gj, c->b.bflag, c->b.use_newton, c->b.Wf, c->b.wcf,
                     c->b.mp, c->b.ctrl, c->b.hist, c->b.err, c->d_keep, c->d_Lt, c->d_P, c->d_x,
                     c->d_rawx, c->d_means, c->d_sphere, c->d_cov, c->d_evwork, c->d_ldetS,
                     c->d_backup, c->d_gradp, c->d_grad};
@@ -434,7 +436,7 @@ int amica_preprocess(amica_ctx* c) {
     CK(cudaSetDevice(c->dev));
     CK(launch_preprocess(c->d_rawx, c->T, c->n, (int)c->cfg.do_sphere, c->d_means, c->d_cov,
                          c->d_sphere, c->d_evwork, c->d_ldetS, c->d_x, c->NP, c->use_tc ? 1 : 0,
-                         c->st));
+                         c->b.err, c->st));
     double ld = 0.0;
     CK(cudaMemcpyAsync(&ld, c->d_ldetS, sizeof(double), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -625,7 +627,7 @@ int amica_set_grid(amica_ctx* c, int64_t max_clusters, int64_t* nclusters) {
     // the partial-sum slots were sized for the largest grid at creation
     if (ncl > c->nclusters_cap) return AMICA_ERR_INVALIDPARAM;
     c->nclusters = ncl;
-    c->nslots = ncl * (c->use_tc ? tc_partial_groups(c->n) : 1);
+    c->nslots = ncl * (c->use_tc ? tc_partial_groups(c->n) : plain_partial_groups(c->n));
     if (c->graph) {
         CK(cudaStreamSynchronize(c->st));
         cudaGraphExecDestroy(c->graph);

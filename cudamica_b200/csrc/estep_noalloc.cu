@@ -18,6 +18,7 @@
 
 namespace amica {
 int plain_pad_channels(int n);
+int plain_partial_groups(int n);
 int plain_max_clusters(int n, int m, int M);
 int plain_tile_samples();
 cudaError_t launch_estep_plain(const EStepArgs& a, int NP, int nclusters, cudaStream_t st);
@@ -63,7 +64,7 @@ __global__ void k_noalloc_ctrl(Ctrl* ctrl, int64_t nkeep) {
 }
 
 // carve the scratch array; returns the bytes needed (0 on overflow of size_t)
-size_t carve(unsigned char* base, int n, int M, int m, int NP, int nclusters, MStepBuffers* b) {
+size_t carve(unsigned char* base, int n, int M, int m, int NP, int nslots, MStepBuffers* b) {
     PartLayout PL{n, m};
     size_t off = 0;
     auto take = [&](size_t bytes) -> unsigned char* {
@@ -78,10 +79,11 @@ size_t carve(unsigned char* base, int n, int M, int m, int NP, int nclusters, MS
     b->Wf = (float*)take(sizeof(float) * M * NP * NP);
     b->wcf = (float*)take(sizeof(float) * M * NP);
     b->mp = (MixParam*)take(sizeof(MixParam) * M * m * NP);
-    b->partial = (double*)take(sizeof(double) * (size_t)nclusters * M * PL.stride());
+    b->partial = (double*)take(sizeof(double) * (size_t)nslots * M * PL.stride());
     b->raw = (double*)take(sizeof(double) * (size_t)M * PL.stride());
     b->ctrl = (Ctrl*)take(sizeof(Ctrl));
     b->err = (int*)take(sizeof(int));
+    if (n > 128) b->gj = (double*)take(sizeof(double) * ((size_t)M * n * n + (size_t)M * n));
     return off;
 }
 
@@ -103,13 +105,15 @@ extern "C" int amica_estep_stats_noalloc(const float* x, int64_t ldx, int64_t n,
     if (ncl <= 0) return AMICA_ERR_UNSUPPORTED;
     if (ncl > kNoAllocMaxClusters) ncl = kNoAllocMaxClusters;
     if (ncl > ntiles) ncl = ntiles;
+    // above 128 channels each cluster has one slot per channel block
+    const int groups = plain_partial_groups((int)n);
     MStepBuffers b;
-    const size_t need = carve(nullptr, (int)n, (int)M, (int)m, NP, ncl, &b);
+    const size_t need = carve(nullptr, (int)n, (int)M, (int)m, NP, ncl * groups, &b);
     if (need > kNoAllocScratchBytes) return AMICA_ERR_UNSUPPORTED;   // beyond the fixed 5 MiB
     unsigned char* base = nullptr;
     int rc = scratch_for_current_device(&base);
     if (rc != AMICA_OK) return rc;
-    carve(base, (int)n, (int)M, (int)m, NP, ncl, &b);
+    carve(base, (int)n, (int)M, (int)m, NP, ncl * groups, &b);
     b.A = const_cast<double*>(A);
     b.c = const_cast<double*>(c);
     b.alpha = const_cast<double*>(alpha);
@@ -129,6 +133,12 @@ extern "C" int amica_estep_stats_noalloc(const float* x, int64_t ldx, int64_t n,
 
     // the only state that must start from zero each call: the error flag
     if (cudaMemsetAsync(b.err, 0, sizeof(int), st) != cudaSuccess) return AMICA_ERR_CUDA;
+    // with channel blocks a slot leaves the other blocks' entries unwritten
+    if (groups > 1) {
+        PartLayout PL{(int)n, (int)m};
+        const size_t pbytes = sizeof(double) * (size_t)ncl * groups * M * PL.stride();
+        if (cudaMemsetAsync(b.partial, 0, pbytes, st) != cudaSuccess) return AMICA_ERR_CUDA;
+    }
     k_noalloc_ctrl<<<1, 1, 0, st>>>(b.ctrl, nkeep);
     if (launch_prep(b, h, st) != cudaSuccess) return AMICA_ERR_CUDA;
     EStepArgs a;
@@ -138,7 +148,7 @@ extern "C" int amica_estep_stats_noalloc(const float* x, int64_t ldx, int64_t n,
     a.T = T; a.ldx = (int)ldx; a.n = (int)n; a.M = (int)M; a.m = (int)m;
     a.ntiles = ntiles; a.nclusters = ncl; a.update_rho = (int)update_rho; a.grad_mode = 0;
     if (launch_estep_plain(a, NP, ncl, st) != cudaSuccess) return AMICA_ERR_CUDA;
-    if (launch_reduce_finalize(b, h, ncl, st) != cudaSuccess) return AMICA_ERR_CUDA;
+    if (launch_reduce_finalize(b, h, ncl * groups, st) != cudaSuccess) return AMICA_ERR_CUDA;
     int herr = 0;
     if (cudaMemcpyAsync(&herr, b.err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return AMICA_ERR_CUDA;

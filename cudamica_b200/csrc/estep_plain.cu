@@ -29,39 +29,48 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kS = 64;  // samples per tile
 
+// NP: channels padded (32, 64, 128 or 256).  Up to 128 channels one CTA per
+// model holds them all; at 256 the Q = 4 CTAs of a model each own NPL = 64
+// channels (their rows of W, their densities, their rows of Psi) and read the
+// full x tile; their per-sample channel sums are added in the cluster.
 template <int NP>
 struct PlainShape {
-    static constexpr int SPLIT = kThreads / NP;     // sample groups per channel
+    static constexpr int NPL = NP <= 128 ? NP : 64; // channels of this CTA
+    static constexpr int Q = NP / NPL;              // CTAs per model
+    static constexpr int SPLIT = kThreads / NPL;    // sample groups per channel
     static constexpr int SUB = kS / SPLIT;          // samples per thread per tile
-    static constexpr int WLD = NP + 4;              // padded row of W^T in smem
+    static constexpr int WLD = NPL + 4;             // padded row of W^T in smem
     static constexpr int XLD = NP + 4;              // padded row of the x tile
     // GEMM b = W x: each thread 4 channels x CT samples
-    static constexpr int NTI = NP / 4;
+    static constexpr int NTI = NPL / 4;
     static constexpr int NTT = kThreads / NTI;
     static constexpr int CT = kS / NTT;
     // Psi update: each thread RI x RK block
-    static constexpr int RI = NP / 16;
+    static constexpr int RI = NPL / 16;
     static constexpr int RK = NP / 16;
-    static constexpr int LLD = NP + 1;              // padded row of the lse tile
-    static constexpr size_t smem_floats = (size_t)NP * WLD + (size_t)kS * XLD + (size_t)kS * NP +
+    static constexpr int LLD = NPL + 1;             // padded row of the lse tile
+    static constexpr size_t smem_floats = (size_t)NP * WLD + (size_t)kS * XLD + (size_t)kS * NPL +
                                           (size_t)kS * LLD + (size_t)kS * LLD + 2 * kS + 2 * kS;
 };
 
 template <int NP, int MM>
 __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     using Sh = PlainShape<NP>;
+    constexpr int NPL = Sh::NPL, Q = Sh::Q;
     extern __shared__ __align__(16) float sm[];
-    float* Wt = sm;                                   // [NP][WLD]  Wt[k][i] = W[i][k]
+    float* Wt = sm;                                   // [NP][WLD]  Wt[k][i] = W[i0 + i][k]
     float* xs = Wt + NP * Sh::WLD;                    // [S][XLD]
-    float* bs = xs + kS * Sh::XLD;                    // [S][NP]    (W x)_i per sample
-    float* gs = bs + kS * NP;                         // [S][NP] g; its region is [S][LLD]
+    float* bs = xs + kS * Sh::XLD;                    // [S][NPL]   (W x)_i per sample
+    float* gs = bs + kS * NPL;                        // [S][NPL] g; its region is [S][LLD]
     float* lse = gs + kS * Sh::LLD;                   // [S][LLD]   log-sum-exp over mixtures
     float* slot = lse + kS * Sh::LLD;                 // [2][S]     cluster-visible L_h(t)
     float* vS = slot + 2 * kS;                        // [S]        v_h(t) (0 if not used)
 
     cg::cluster_group cluster = cg::this_cluster();
-    const int h = (int)cluster.block_rank();
-    const int cid = blockIdx.x / a.M;
+    const int rank = (int)cluster.block_rank();
+    const int h = rank / Q, cq = rank % Q;            // model, channel block
+    const int i0c = cq * NPL;                         // first channel of this CTA
+    const int cid = blockIdx.x / (a.M * Q);
     const int tid = threadIdx.x;
     const int n = a.n, M = a.M;
     if (a.m != MM || n > NP) {
@@ -69,14 +78,15 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     }
 
     // ---- resident per-CTA data: W_h^T and this thread's mixture constants
-    const float* Wh = a.Wf + (size_t)h * NP * NP;
-    for (int e = tid; e < NP * NP; e += kThreads) {
+    const float* Wh = a.Wf + ((size_t)h * NP + i0c) * NP;
+    for (int e = tid; e < NPL * NP; e += kThreads) {
         int i = e / NP, k = e % NP;
         Wt[k * Sh::WLD + i] = Wh[e];
     }
-    const int ch = tid % NP;            // density-phase channel
-    const int grp = tid / NP;           // density-phase sample group
-    const bool ch_ok = ch < n;
+    const int ch = tid % NPL;           // density-phase channel (of this CTA)
+    const int grp = tid / NPL;          // density-phase sample group
+    const int gch = i0c + ch;           // the channel's index in the model
+    const bool ch_ok = gch < n;
     // mixtures (0,1), (2,3) as float2 pairs, an odd last one as a scalar
     constexpr int NPR = MM / 2;
     constexpr bool kOdd = (MM & 1) != 0;
@@ -86,7 +96,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     MixV<float> P1;
 #pragma unroll
     for (int j = 0; j < MM; j++) {
-        const MixParam q = a.mp[((size_t)h * MM + j) * NP + ch];
+        const MixParam q = a.mp[((size_t)h * MM + j) * NP + gch];
         pr[j] = q.rho;
         if (j < 2 * NPR) {
             float2* f[5] = {&P2[j / 2].s, &P2[j / 2].npo, &P2[j / 2].pc, &P2[j / 2].pr, &P2[j / 2].sr};
@@ -100,7 +110,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
             P1.s = q.s; P1.npo = -q.off; P1.pc = q.cl2; P1.pr = q.rho; P1.sr = q.s * q.rho;
         }
     }
-    const float wci = a.wc[(size_t)h * NP + ch];
+    const float wci = a.wc[(size_t)h * NP + gch];
     float ltc[kMaxModels];
 #pragma unroll
     for (int q = 0; q < kMaxModels; q++) ltc[q] = (q < M) ? (float)(a.ltc64[q] - a.ltc64[0]) : 0.f;
@@ -159,7 +169,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
             }
 #pragma unroll
             for (int c = 0; c < Sh::CT; c++)
-                *reinterpret_cast<float4*>(bs + (tt * Sh::CT + c) * NP + 4 * ti) =
+                *reinterpret_cast<float4*>(bs + (tt * Sh::CT + c) * NPL + 4 * ti) =
                     make_float4(acc[c][0], acc[c][1], acc[c][2], acc[c][3]);
         }
         __syncthreads();
@@ -167,7 +177,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
 #pragma unroll 4
         for (int r = 0; r < Sh::SUB; r++) {
             const int t = grp * Sh::SUB + r;
-            const float bx = bs[t * NP + ch];
+            const float bx = bs[t * NPL + ch];
             float q[MM];
 #pragma unroll
             for (int qq = 0; qq < NPR; qq++) {
@@ -183,11 +193,17 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
         }
         __syncthreads();
         // ---- Lt_h(t): channel sum in fixed order, published for the cluster
+        // (with Q > 1, this CTA's channels only; the blocks are added below)
         float* myslot = slot + par * kS;
         if (tid < kS) {
             float s = 0.f;
-            for (int i = 0; i < n; i++) s += lse[tid * Sh::LLD + i];
-            myslot[tid] = ltc[h] + kLn2 * s;
+            if constexpr (Q == 1) {
+                for (int i = 0; i < n; i++) s += lse[tid * Sh::LLD + i];
+                myslot[tid] = ltc[h] + kLn2 * s;
+            } else {
+                for (int i = 0; i < NPL; i++) s += lse[tid * Sh::LLD + i];
+                myslot[tid] = s;
+            }
         }
         cluster.sync();
         // ---- P(t) and v_h(t) (identical arithmetic in every CTA of the cluster)
@@ -197,8 +213,15 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
 #pragma unroll
             for (int q = 0; q < kMaxModels; q++) {
                 if (q < M) {
-                    const float* ps_q = cluster.map_shared_rank(myslot, q);
-                    L[q] = ps_q[tid];
+                    if constexpr (Q == 1) {
+                        const float* ps_q = cluster.map_shared_rank(myslot, q);
+                        L[q] = ps_q[tid];
+                    } else {
+                        float s = 0.f;
+#pragma unroll
+                        for (int b = 0; b < Q; b++) s += cluster.map_shared_rank(myslot, q * Q + b)[tid];
+                        L[q] = ltc[q] + kLn2 * s;
+                    }
                     lmax = fmaxf(lmax, L[q]);
                 }
             }
@@ -211,11 +234,11 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
             const int64_t tg = t0 + tid;
             const bool valid = tg < a.T && (a.keep == nullptr || a.keep[tg]);
             vS[tid] = valid ? vh : 0.f;
-            if (valid) {
+            if (valid && cq == 0) {
                 dVs += (double)vh;
                 if (h == 0) dLL += (double)P;
             }
-            if (tg < a.T) {
+            if (tg < a.T && cq == 0) {
                 if (a.Lt_out) a.Lt_out[(size_t)h * a.T + tg] = L[h];
                 if (a.P_out && h == 0) a.P_out[tg] = P;
             }
@@ -236,7 +259,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
             for (int r = 0; r < Sh::SUB; r++) {
                 const int t = grp * Sh::SUB + r;
                 const float v = vS[t];
-                const float bx = bs[t * NP + ch];
+                const float bx = bs[t * NPL + ch];
                 const float nl = -lse[t * Sh::LLD + ch];
                 float2 g2 = make_float2(0.f, 0.f);
                 float g1 = 0.f;
@@ -249,7 +272,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
                 fCn = fmaf(v, bb, fCn);          // sum v b; cnew = A sum(v b) / vsum + c
                 fS2 = fmaf(v * bb, bb, fS2);
                 fGs += ch_ok ? g : 0.f;
-                gs[t * NP + ch] = ch_ok ? g : 0.f;
+                gs[t * NPL + ch] = ch_ok ? g : 0.f;
             }
             if (ch_ok) {
 #pragma unroll
@@ -273,7 +296,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
             for (int t = 0; t < kS; t++) {
                 float gv[Sh::RI], xv[Sh::RK];
 #pragma unroll
-                for (int r = 0; r < Sh::RI; r++) gv[r] = gs[t * NP + i0 + r];
+                for (int r = 0; r < Sh::RI; r++) gv[r] = gs[t * NPL + i0 + r];
 #pragma unroll
                 for (int c = 0; c < Sh::RK; c++) xv[c] = xs[t * Sh::XLD + k0 + c];
 #pragma unroll
@@ -287,8 +310,9 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
 
     // ---- write this CTA's partial sums (fixed-order combination of groups)
     PartLayout L{n, MM};
-    double* out = a.partial + ((size_t)cid * M + h) * L.stride();
-    double* red = reinterpret_cast<double*>(xs);   // [SPLIT][NP] doubles, one statistic at a time
+    // one slot per (cluster, channel block); entries of the other blocks stay zero
+    double* out = a.partial + ((size_t)(cid * Q + cq) * M + h) * L.stride();
+    double* red = reinterpret_cast<double*>(xs);   // [SPLIT][NPL] doubles, one statistic at a time
     constexpr int NACC = 7 * MM + 3;
     double vals[NACC];
 #pragma unroll
@@ -301,16 +325,17 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     vals[7 * MM + 0] = dCn; vals[7 * MM + 1] = dS2; vals[7 * MM + 2] = dGs;
 #pragma unroll
     for (int k = 0; k < NACC; k++) {
-        red[grp * NP + ch] = vals[k];
+        red[grp * NPL + ch] = vals[k];
         __syncthreads();
-        if (tid < NP && tid < n) {
+        if (tid < NPL && i0c + tid < n) {
             double s = 0.0;
-            for (int g2 = 0; g2 < Sh::SPLIT; g2++) s += red[g2 * NP + tid];
+            for (int g2 = 0; g2 < Sh::SPLIT; g2++) s += red[g2 * NPL + tid];
+            const int gi = i0c + tid;
             int dst;
-            if (k < 7 * MM) dst = L.mix(k / MM) + (k % MM) * n + tid;
-            else if (k == 7 * MM) dst = L.cn() + tid;
-            else if (k == 7 * MM + 1) dst = L.s2() + tid;
-            else dst = L.gs() + tid;
+            if (k < 7 * MM) dst = L.mix(k / MM) + (k % MM) * n + gi;
+            else if (k == 7 * MM) dst = L.cn() + gi;
+            else if (k == 7 * MM + 1) dst = L.s2() + gi;
+            else dst = L.gs() + gi;
             out[dst] = s;
         }
         __syncthreads();
@@ -319,7 +344,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     double* red2 = red;
     if (tid < kS) { red2[tid] = dLL; red2[kS + tid] = dVs; }
     __syncthreads();
-    if (tid == 0) {
+    if (tid == 0 && cq == 0) {
         double s0 = 0.0, s1 = 0.0;
         for (int t = 0; t < kS; t++) { s0 += red2[t]; s1 += red2[kS + t]; }
         out[0] = s0;
@@ -332,7 +357,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
         for (int r = 0; r < Sh::RI; r++)
 #pragma unroll
             for (int c = 0; c < Sh::RK; c++) {
-                const int i = i0 + r, k = k0 + c;
+                const int i = i0c + i0 + r, k = k0 + c;
                 if (i < n && k < n) out[L.psi() + (size_t)k * n + i] = (double)psi[r][c];
             }
     }
@@ -347,18 +372,18 @@ cudaError_t launch_plain(const EStepArgs& a, int nclusters, cudaStream_t st) {
     auto kern = estep_plain_kernel<NP, MM>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    if (a.M > 1) {
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 0);
+    if (a.M * Sh::Q > 1) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         if (e != cudaSuccess) return e;
     }
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(nclusters * a.M);
+    cfg.gridDim = dim3(nclusters * a.M * Sh::Q);
     cfg.blockDim = dim3(kThreads);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = a.M;
+    attr[0].val.clusterDim.x = a.M * Sh::Q;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
@@ -372,7 +397,11 @@ namespace amica {
 
 int plain_tile_samples() { return kS; }
 
-int plain_pad_channels(int n) { return n <= 32 ? 32 : (n <= 64 ? 64 : (n <= 128 ? 128 : -1)); }
+int plain_pad_channels(int n) {
+    return n <= 32 ? 32 : (n <= 64 ? 64 : (n <= 128 ? 128 : (n <= 256 ? 256 : -1)));
+}
+// Partial-sum slots per cluster: one per channel block.
+int plain_partial_groups(int n) { return plain_pad_channels(n) == 256 ? PlainShape<256>::Q : 1; }
 
 // Largest cluster count whose clusters can all be resident at once (the grid
 // is persistent: every cluster loops over its share of the tiles).
@@ -383,13 +412,17 @@ int max_active_clusters(int M) {
     auto kern = estep_plain_kernel<NP, MM>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return -1;
+    const int csize = M * Sh::Q;
+    if (csize > 8 &&
+        cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+        return -1;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(M * 64);
+    cfg.gridDim = dim3(csize * 64);
     cfg.blockDim = dim3(kThreads);
     cfg.dynamicSmemBytes = smem;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = M;
+    attr[0].val.clusterDim.x = csize;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
@@ -413,6 +446,7 @@ int plain_max_clusters(int n, int m, int M) {
     AMICA_PLAIN_OCC_NP(32)
     AMICA_PLAIN_OCC_NP(64)
     AMICA_PLAIN_OCC_NP(128)
+    AMICA_PLAIN_OCC_NP(256)
 #undef AMICA_PLAIN_OCC_NP
 #undef AMICA_PLAIN_OCC
     return -1;
@@ -427,6 +461,7 @@ cudaError_t launch_estep_plain(const EStepArgs& a, int NP, int nclusters, cudaSt
     AMICA_PLAIN_NP(32)
     AMICA_PLAIN_NP(64)
     AMICA_PLAIN_NP(128)
+    AMICA_PLAIN_NP(256)
 #undef AMICA_PLAIN_NP
 #undef AMICA_PLAIN_CASE
     return cudaErrorInvalidValue;

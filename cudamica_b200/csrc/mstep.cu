@@ -216,6 +216,140 @@ __global__ void __launch_bounds__(kInvThreads, 1) k_inverse_derive(
     }
 }
 
+// ---------------------------------------------------------------------------
+// k_inverse_gj: W_h = A_h^{-1} and log|pivots| for 128 < n <= 256, where the
+// n x n FP64 matrix no longer fits in one SM.  The same Gauss-Jordan
+// elimination as k_inverse_derive (partial pivoting, no row interchanges,
+// largest |a(r, k)| over the unused rows, lowest row on ties, exact compares)
+// on a column-major working copy in global memory (L2-resident); one CTA of
+// 1024 threads per model, the pivot column and row staged in shared memory.
+constexpr int kGJThreads = 1024;
+constexpr int kMaxN = 256;
+__global__ void __launch_bounds__(kGJThreads, 1) k_inverse_gj(const double* __restrict__ A,
+                                                             double* __restrict__ work,
+                                                             double* __restrict__ W,
+                                                             double* __restrict__ pivlog, int n,
+                                                             int* err) {
+    const int h = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* a = work + (size_t)h * n * n;
+    const double* Ah = A + (size_t)h * n * n;
+    __shared__ double f[kMaxN], prow[kMaxN], wv[32];
+    __shared__ int perm[kMaxN], pinv[kMaxN], wi[32];
+    __shared__ unsigned char used[kMaxN];
+    __shared__ int s_p, s_bad;
+    __shared__ double s_inv;
+    for (int e = tid; e < n * n; e += kGJThreads) a[e] = Ah[e];
+    for (int i = tid; i < n; i += kGJThreads) used[i] = 0;
+    if (tid == 0) s_bad = 0;
+    __syncthreads();
+    for (int k = 0; k < n; k++) {
+        double v = -1.0;
+        int r = 0x7fffffff;
+        if (tid < n && !used[tid]) { v = fabs(a[(size_t)k * n + tid]); r = tid; }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+            const int r2 = __shfl_xor_sync(0xffffffffu, r, o);
+            if (v2 > v || (v2 == v && r2 < r)) { v = v2; r = r2; }
+        }
+        if (lane == 0) { wv[warp] = v; wi[warp] = r; }
+        __syncthreads();
+        if (tid == 0) {
+            double bv = wv[0];
+            int br = wi[0];
+            for (int q = 1; q < kGJThreads / 32; q++)
+                if (wv[q] > bv || (wv[q] == bv && wi[q] < br)) { bv = wv[q]; br = wi[q]; }
+            if (!(bv > 0.0)) {
+                s_bad = 1;
+            } else {
+                const double piv = a[(size_t)k * n + br];
+                s_p = br;
+                s_inv = 1.0 / piv;
+                perm[k] = br;
+                pinv[br] = k;
+                used[br] = 1;
+                pivlog[(size_t)h * n + k] = log(fabs(piv));
+            }
+        }
+        __syncthreads();
+        if (s_bad) break;
+        const int p = s_p;
+        const double inv = s_inv;
+        if (tid < n) {
+            f[tid] = a[(size_t)k * n + tid];
+            prow[tid] = a[(size_t)tid * n + p];
+        }
+        __syncthreads();
+        for (int e = tid; e < n * n; e += kGJThreads) {
+            const int j = e / n, rr = e - j * n;
+            if (j == k) a[e] = (rr == p) ? inv : -f[rr] * inv;
+            else if (rr == p) a[e] = prow[j] * inv;
+            else a[e] = fma(-f[rr], prow[j] * inv, a[e]);
+        }
+        __syncthreads();
+    }
+    if (s_bad) {
+        if (tid == 0) atomicOr(err, kErrSingular);
+        return;
+    }
+    // W(j, p_k) = a(p_j, k), W column-major
+    double* Wh = W + (size_t)h * n * n;
+    for (int e = tid; e < n * n; e += kGJThreads) {
+        const int k = e / n, rr = e - k * n;
+        Wh[(size_t)perm[k] * n + pinv[rr]] = a[e];
+    }
+}
+
+// k_derive: log|det W_h|, the Lt constant and the FP32 E-step constants from a
+// column-major W (the tail of k_inverse_derive for the n > 128 path).  One CTA
+// of 256 threads per model.
+__global__ void __launch_bounds__(256) k_derive(
+    const double* __restrict__ W, const double* __restrict__ pivlog, const double* __restrict__ c,
+    const double* __restrict__ alpha, const double* __restrict__ mu, const double* __restrict__ beta,
+    const double* __restrict__ rho, const double* __restrict__ gm, double ldetS,
+    double* __restrict__ ldet, double* __restrict__ ltc64, float* __restrict__ Wf,
+    float* __restrict__ wcf, MixParam* __restrict__ mp, int n, int m, int NP) {
+    const int h = blockIdx.x, tid = threadIdx.x;
+    const double* Wh = W + (size_t)h * n * n;
+    __shared__ double wcs[kMaxN];
+    if (tid == 0) {
+        double ld = 0.0;
+        for (int k = 0; k < n; k++) ld += pivlog[(size_t)h * n + k];
+        ldet[h] = -ld;
+        ltc64[h] = log(gm[h]) - ld + ldetS;           // src/amica.cu:1009
+    }
+    for (int i = tid; i < NP; i += blockDim.x) {
+        double wc = 0.0;
+        if (i < n)
+            for (int k = 0; k < n; k++) wc += Wh[(size_t)k * n + i] * c[(size_t)h * n + k];
+        wcs[i] = wc;
+        wcf[(size_t)h * NP + i] = (float)wc;
+    }
+    float* Wfh = Wf + (size_t)h * NP * NP;
+    for (int e = tid; e < NP * NP; e += blockDim.x) {
+        const int i = e / NP, k = e - i * NP;
+        Wfh[e] = (i < n && k < n) ? (float)Wh[(size_t)k * n + i] : 0.f;
+    }
+    __syncthreads();
+    for (int e = tid; e < m * NP; e += blockDim.x) {
+        const int j = e / NP, i = e - j * NP;
+        MixParam q;
+        if (i < n) {
+            const size_t idx = ((size_t)h * m + j) * n + i;
+            const double s = sqrt(beta[idx]);
+            const double r = rho[idx];
+            q.s = (float)s;
+            q.off = (float)(s * (mu[idx] + wcs[i]));
+            q.cl2 = (float)((log(alpha[idx]) + 0.5 * log(beta[idx]) - M_LN2 - lgamma(1.0 + 1.0 / r)) *
+                            1.4426950408889634);
+            q.rho = (float)r;
+        } else {
+            q.s = 0.f; q.off = 0.f; q.cl2 = 0.f; q.rho = 1.f;
+        }
+        mp[((size_t)h * m + j) * NP + i] = q;
+    }
+}
+
 // Entry (r, cc) of the A-update matrix B_h (src/amica.cu:2155-2279,
 // src/kernels.cu:961-1014): the Newton form when this model takes the Newton
 // step, else the natural gradient I - phi / vsum.
@@ -311,7 +445,7 @@ __global__ void __launch_bounds__(256) k_gemm64(GemmArgs g) {
 
 // Reparametrisation and c update after the A update (src/amica.cu:2367-2512):
 // unit columns of A, mu *= norm, beta /= norm^2, mu -= W_old (cnew - c), c = cnew.
-// One CTA of 1024 threads per model (n <= 128).
+// One CTA of 1024 threads per model (n <= 256).
 __global__ void __launch_bounds__(1024) k_reparm(int update_A, int do_reparm, double* A,
                                                  const double* __restrict__ Anew,
                                                  const double* __restrict__ W, double* c,
@@ -320,7 +454,7 @@ __global__ void __launch_bounds__(1024) k_reparm(int update_A, int do_reparm, do
     const int h = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const double* cnew = work + (size_t)h * 4 * n + 3 * n;
     double* ch = c + (size_t)h * n;
-    __shared__ double norms[128], shift[128], dc[128];
+    __shared__ double norms[kMaxN], shift[kMaxN], dc[kMaxN];
     if (update_A) {
         double* Ah = A + (size_t)h * n * n;
         const double* An = Anew + (size_t)h * n * n;
@@ -333,8 +467,8 @@ __global__ void __launch_bounds__(1024) k_reparm(int update_A, int do_reparm, do
             }
             if (tid < n) dc[tid] = cnew[tid] - ch[tid];
             __syncthreads();
-            {
-                const int i = tid >> 3, part = tid & 7;
+            for (int ib = 0; ib < n; ib += 128) {
+                const int i = ib + (tid >> 3), part = tid & 7;
                 const double* Wh = W + (size_t)h * n * n;
                 double acc = 0.0;
                 if (i < n)
@@ -345,10 +479,9 @@ __global__ void __launch_bounds__(1024) k_reparm(int update_A, int do_reparm, do
                 if (part == 0 && i < n) shift[i] = acc;
             }
             __syncthreads();
-            for (int cc = tid >> 7; cc < n; cc += 8) {
-                const int r = tid & 127;
-                if (r < n) Ah[(size_t)cc * n + r] = An[(size_t)cc * n + r] / norms[cc];
-            }
+            for (int cc = tid >> 7; cc < n; cc += 8)
+                for (int r = tid & 127; r < n; r += 128)
+                    Ah[(size_t)cc * n + r] = An[(size_t)cc * n + r] / norms[cc];
             for (int e = tid; e < m * n; e += blockDim.x) {
                 const int i = e % n;
                 const size_t idx = (size_t)h * m * n + e;
@@ -471,13 +604,12 @@ __global__ void __launch_bounds__(kMT) k_mstep_params(
     double* sig2 = kappa + 2 * n;
     double* cnew = kappa + 3 * n;
     __shared__ double sh[33];
-    __shared__ double ks[128];
+    __shared__ double ks[kMaxN];
     const double vsum = S[SL.vs()];
     const double ivs = 1.0 / vsum;
     if (tid == 0 && cf.update_gm) gm[h] = vsum / Tk;
     // alpha = usum / vsum; then kappa / lambda with the new alpha and old mu
-    if (tid < n) {
-        const int i = tid;
+    for (int i = tid; i < n; i += kMT) {
         const double s2 = S[SL.s2() + i] * ivs;
         sig2[i] = s2;
         cnew[i] = S[SL.cn() + i] * ivs;
@@ -518,12 +650,9 @@ __global__ void __launch_bounds__(kMT) k_mstep_params(
     if (!cf.update_A) return;
     // bflag: entries of (kappa sigma2)(kappa sigma2)^T that are <= 1, diagonal included
     double cnt = 0.0;
-    {
-        const int r = tid & 127;
-        if (r < n)
-            for (int cc = tid >> 7; cc < n; cc += kMT / 128)
-                if (ks[r] * ks[cc] <= 1.0) cnt += 1.0;
-    }
+    for (int r = tid & 127; r < n; r += 128)
+        for (int cc = tid >> 7; cc < n; cc += kMT / 128)
+            if (ks[r] * ks[cc] <= 1.0) cnt += 1.0;
     cnt = block_sum(cnt, sh);
     const int64_t bf = (int64_t)cnt;
     const int newton = (bf == 0 && cf.do_newton && iter >= cf.newt_start_iter);
@@ -680,7 +809,15 @@ static MCfg to_mcfg(const MStepCfgHost& h) {
 }
 
 cudaError_t launch_prep(const MStepBuffers& b, const MStepCfgHost& h, cudaStream_t st) {
-    if (h.n > 128) return cudaErrorInvalidValue;
+    if (h.n > kMaxN) return cudaErrorInvalidValue;
+    if (h.n > 128) {
+        if (!b.gj) return cudaErrorInvalidValue;
+        double* pivlog = b.gj + (size_t)h.M * h.n * h.n;
+        k_inverse_gj<<<h.M, kGJThreads, 0, st>>>(b.A, b.gj, b.W, pivlog, h.n, b.err);
+        k_derive<<<h.M, 256, 0, st>>>(b.W, pivlog, b.c, b.alpha, b.mu, b.beta, b.rho, b.gm, h.ldetS,
+                                      b.ldet, b.ltc64, b.Wf, b.wcf, b.mp, h.n, h.m, h.NP);
+        return cudaGetLastError();
+    }
     const size_t smem = sizeof(double) * (size_t)h.n * h.n;
     cudaError_t e = cudaFuncSetAttribute(k_inverse_derive, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);

@@ -306,6 +306,281 @@ __global__ void __launch_bounds__(kJacThreads, 1) k_jacobi_smem(const double* __
     for (int i = tid; i < n; i += kJacThreads) evals[i] = ap[pk_idx(i, i)];
 }
 
+// ---------------------------------------------------------------------------
+// 128 < n <= 256.  The n <= 128 kernels keep the whole problem in one SM; here
+// the covariance runs k_cov8's register blocking on the four 128 x 128
+// quadrants, the eigendecomposition spreads the same Jacobi rounds over a
+// cooperative grid, and the sphering keeps a 64-row slice of S per CTA.
+
+// k_cov8 for the quadrant (oi, ok) of C (rows oi .., columns ok ..): blockIdx.y
+// selects the quadrant; both 128-channel sample slices are staged.
+__global__ void __launch_bounds__(256, 1) k_cov8q(const float* __restrict__ x, int64_t T, int n,
+                                                  int64_t chunk, const double* __restrict__ mean,
+                                                  double* __restrict__ part) {
+    extern __shared__ __align__(16) double cq[];
+    double (*xi_s)[128] = reinterpret_cast<double (*)[128]>(cq);
+    double (*xk_s)[128] = reinterpret_cast<double (*)[128]>(cq + kCovRows * 128);
+    const int oi = 128 * (blockIdx.y & 1), ok = 128 * (blockIdx.y >> 1);
+    const int bi = threadIdx.x & 15, bk = threadIdx.x >> 4;
+    const int64_t t0 = (int64_t)blockIdx.x * chunk;
+    const int64_t t1 = t0 + chunk < T ? t0 + chunk : T;
+    double acc[8][8];
+#pragma unroll
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int b = 0; b < 8; b++) acc[a][b] = 0.0;
+    for (int64_t tb = t0; tb < t1; tb += kCovRows) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < kCovRows * 128; e += 256) {
+            const int r = e >> 7, i = e & 127;
+            const int64_t t = tb + r;
+            const bool in = t < t1;
+            xi_s[r][i] = (in && oi + i < n) ? (double)x[t * n + oi + i] - mean[oi + i] : 0.0;
+            xk_s[r][i] = (in && ok + i < n) ? (double)x[t * n + ok + i] - mean[ok + i] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 2
+        for (int r = 0; r < kCovRows; r++) {
+            double xi[8], xk[8];
+#pragma unroll
+            for (int a = 0; a < 8; a += 2) {
+                const double2 u = *reinterpret_cast<const double2*>(&xi_s[r][8 * bi + a]);
+                const double2 w = *reinterpret_cast<const double2*>(&xk_s[r][8 * bk + a]);
+                xi[a] = u.x; xi[a + 1] = u.y; xk[a] = w.x; xk[a + 1] = w.y;
+            }
+#pragma unroll
+            for (int a = 0; a < 8; a++)
+#pragma unroll
+                for (int b = 0; b < 8; b++) acc[a][b] = fma(xi[a], xk[b], acc[a][b]);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const int i = oi + 8 * bi + a, k = ok + 8 * bk + b;
+            if (i < n && k < n) part[(size_t)blockIdx.x * n * n + (size_t)k * n + i] = acc[a][b];
+        }
+}
+
+// Grid-wide barrier for a cooperative launch: a monotonic arrival counter;
+// barrier number b completes when it reaches (b + 1) * gridDim.x.  The wait is
+// bounded (~1 s); on expiry it records kErrWaitTimeout and sets *abort, after
+// which every block leaves its loops at the next barrier.
+__device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned target, volatile int* abort,
+                                             int* err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(count, 1u);
+        const long long t0 = clock64();
+        while (true) {
+            const unsigned v = *(volatile unsigned*)count;
+            if (v >= target || *abort) break;
+            if (clock64() - t0 > 2000000000LL) {
+                *abort = 1;
+                atomicOr(err, amica::kErrWaitTimeout);
+                break;
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *abort == 0;
+}
+
+// The Jacobi eigendecomposition of k_jacobi_smem (same round-robin schedule,
+// rotation formula, 2 x 2 block transforms, eigenvector update and stopping
+// rule) with the packed triangle and V in global memory, rounds spread over all
+// blocks of a cooperative launch: every block forms the round's n/2 rotations
+// from the packed triangle, a grid barrier, the blocks share out the 2 x 2 block
+// and V updates, and a second grid barrier ends the round.  Loads of shared
+// state bypass L1.
+struct JacGlobal {
+    double* ap;        // packed upper triangle, n (n + 1) / 2
+    double* part;      // per-block partial sums of the stopping test, 2 per block
+    unsigned* count;   // barrier counter (zero at launch)
+    int* abort;        // zero at launch
+};
+__global__ void __launch_bounds__(kJacThreads, 1) k_jacobi_grid(const double* __restrict__ C,
+                                                                double* __restrict__ V,
+                                                                double* __restrict__ evals, int n,
+                                                                JacGlobal g, int* err) {
+    __shared__ double cs[128], sn[128];
+    __shared__ int pp[128], qq[128];
+    __shared__ double red[32];
+    const int tid = threadIdx.x;
+    const int gtid = blockIdx.x * kJacThreads + tid, gthreads = gridDim.x * kJacThreads;
+    const int np = (n * (n + 1)) / 2;
+    const int ne = n + (n & 1), half = ne / 2;
+    const int nblk = half * (half + 1) / 2;
+    double* ap = g.ap;
+    unsigned bar = 0;
+    for (int e = gtid; e < n * n; e += gthreads) {
+        const int r = e % n, c = e / n;
+        if (r <= c) ap[pk_idx(r, c)] = C[e];
+        V[e] = (r == c) ? 1.0 : 0.0;
+    }
+    if (!grid_barrier(g.count, (++bar) * gridDim.x, g.abort, err)) return;
+    for (int sweep = 0; sweep < 40; sweep++) {
+        double off = 0.0, tot = 0.0;
+        for (int e = gtid; e < np; e += gthreads) {
+            int j = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+            while (pk_idx(0, j + 1) <= e) j++;
+            while (pk_idx(0, j) > e) j--;
+            const double v = __ldcg(ap + e);
+            const bool diag = (e - pk_idx(0, j)) == j;
+            tot += diag ? v * v : 2.0 * v * v;
+            off += diag ? 0.0 : 2.0 * v * v;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            off += __shfl_xor_sync(0xffffffffu, off, o);
+            tot += __shfl_xor_sync(0xffffffffu, tot, o);
+        }
+        if ((tid & 31) == 0) red[tid >> 5] = off;
+        __syncthreads();
+        if (tid == 0) {
+            double s = 0.0;
+            for (int w = 0; w < kJacThreads / 32; w++) s += red[w];
+            g.part[2 * blockIdx.x] = s;
+        }
+        __syncthreads();
+        if ((tid & 31) == 0) red[tid >> 5] = tot;
+        __syncthreads();
+        if (tid == 0) {
+            double s = 0.0;
+            for (int w = 0; w < kJacThreads / 32; w++) s += red[w];
+            g.part[2 * blockIdx.x + 1] = s;
+        }
+        if (!grid_barrier(g.count, (++bar) * gridDim.x, g.abort, err)) return;
+        // every block sums the partials in the same order and takes the same decision
+        double offt = 0.0, tott = 0.0;
+        for (int b = 0; b < (int)gridDim.x; b++) {
+            offt += __ldcg(g.part + 2 * b);
+            tott += __ldcg(g.part + 2 * b + 1);
+        }
+        if (offt <= 1e-30 * tott) break;
+        // the partials are rewritten next sweep only after every block has read
+        // them: the first round's barrier lies in between
+        for (int round = 0; round < ne - 1; round++) {
+            if (tid < half) {
+                auto pos = [&](int j) { return j == 0 ? 0 : 1 + ((j - 1 + round) % (ne - 1)); };
+                int p = pos(tid), q = pos(ne - 1 - tid);
+                if (p > q) { const int t = p; p = q; q = t; }
+                double c = 1.0, s = 0.0;
+                if (q < n) {
+                    const double apq = __ldcg(ap + pk_idx(p, q));
+                    if (fabs(apq) >= 1e-300) {
+                        const double app = __ldcg(ap + pk_idx(p, p)), aqq = __ldcg(ap + pk_idx(q, q));
+                        const double th = (aqq - app) / (2.0 * apq);
+                        const double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+                        c = 1.0 / sqrt(t * t + 1.0);
+                        s = t * c;
+                    }
+                }
+                pp[tid] = p; qq[tid] = q; cs[tid] = c; sn[tid] = s;
+            }
+            // every block has read the diagonal entries that the round's K = L
+            // blocks are about to overwrite
+            if (!grid_barrier(g.count, (++bar) * gridDim.x, g.abort, err)) return;
+            // A <- J^T A J: block (K, L), K <= L, numbered column by column
+            for (int e = gtid; e < nblk; e += gthreads) {
+                int L = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+                while ((L + 1) * (L + 2) / 2 <= e) L++;
+                while (L * (L + 1) / 2 > e) L--;
+                const int K = e - L * (L + 1) / 2;
+                const int pK = pp[K], qK = qq[K], pL = pp[L], qL = qq[L];
+                const double cK = cs[K], sK = sn[K], cL = cs[L], sL = sn[L];
+                if (K == L) {
+                    if (qK < n && sK != 0.0) {
+                        const double app = __ldcg(ap + pk_idx(pK, pK)), aqq = __ldcg(ap + pk_idx(qK, qK));
+                        const double apq = __ldcg(ap + pk_idx(pK, qK));
+                        ap[pk_idx(pK, pK)] = cK * cK * app - 2.0 * cK * sK * apq + sK * sK * aqq;
+                        ap[pk_idx(qK, qK)] = sK * sK * app + 2.0 * cK * sK * apq + cK * cK * aqq;
+                        ap[pk_idx(pK, qK)] = 0.0;
+                    }
+                    continue;
+                }
+                if (sK == 0.0 && sL == 0.0) continue;
+                const bool hq = qK < n, hqL = qL < n;
+                const double b11 = __ldcg(ap + pk_sym(pK, pL));
+                const double b12 = hqL ? __ldcg(ap + pk_sym(pK, qL)) : 0.0;
+                const double b21 = hq ? __ldcg(ap + pk_sym(qK, pL)) : 0.0;
+                const double b22 = (hq && hqL) ? __ldcg(ap + pk_sym(qK, qL)) : 0.0;
+                const double d11 = cL * b11 - sL * b12, d12 = sL * b11 + cL * b12;
+                const double d21 = cL * b21 - sL * b22, d22 = sL * b21 + cL * b22;
+                ap[pk_sym(pK, pL)] = cK * d11 - sK * d21;
+                if (hqL) ap[pk_sym(pK, qL)] = cK * d12 - sK * d22;
+                if (hq) ap[pk_sym(qK, pL)] = sK * d11 + cK * d21;
+                if (hq && hqL) ap[pk_sym(qK, qL)] = sK * d12 + cK * d22;
+            }
+            // V <- V J, one (rotation, row) pair per work item
+            for (int e = gtid; e < half * n; e += gthreads) {
+                const int k = e / n, r = e - k * n;
+                const int p = pp[k], q = qq[k];
+                const double s = sn[k];
+                if (q >= n || s == 0.0) continue;
+                const double c = cs[k];
+                const double vp = __ldcg(V + (size_t)p * n + r), vq = __ldcg(V + (size_t)q * n + r);
+                V[(size_t)p * n + r] = c * vp - s * vq;
+                V[(size_t)q * n + r] = s * vp + c * vq;
+            }
+            if (!grid_barrier(g.count, (++bar) * gridDim.x, g.abort, err)) return;
+        }
+    }
+    for (int i = gtid; i < n; i += gthreads) evals[i] = __ldcg(ap + pk_idx(i, i));
+}
+
+// x_out[t][i] for 128 < n <= 256: blockIdx.y picks 64 output channels whose
+// rows of S stay in shared memory; 16-sample tiles, one (sample, 2 channels)
+// per thread; the same k-ascending FMA order as k_apply_sphere8.
+constexpr int kSphTileQ = 16;
+__global__ void __launch_bounds__(512, 1) k_apply_sphere_q(const float* __restrict__ x, int64_t T,
+                                                           int n, const double* __restrict__ mean,
+                                                           const double* __restrict__ S,
+                                                           float* __restrict__ xo, int ldx, int tf32) {
+    extern __shared__ __align__(16) double sq[];
+    double* Sq = sq;                                   // [256][64]: S(i0 + il, k) at k * 64 + il
+    double* xc = sq + 256 * 64;                        // [16][257]
+    constexpr int XL = 257;
+    const int i0 = 64 * blockIdx.y;
+    for (int e = threadIdx.x; e < 256 * 64; e += 512) {
+        const int k = e >> 6, il = e & 63, i = i0 + il;
+        Sq[e] = (i < n && k < n) ? S[(size_t)k * n + i] : 0.0;
+    }
+    const int s = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t ntile = (T + kSphTileQ - 1) / kSphTileQ;
+    for (int64_t tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+        const int64_t t0 = tile * kSphTileQ;
+        __syncthreads();
+        for (int e = threadIdx.x; e < kSphTileQ * 256; e += 512) {
+            const int r = e >> 8, k = e & 255;
+            const int64_t t = t0 + r;
+            xc[r * XL + k] = (t < T && k < n) ? (double)x[t * n + k] - mean[k] : 0.0;
+        }
+        __syncthreads();
+        double acc0 = 0.0, acc1 = 0.0;
+#pragma unroll 4
+        for (int k = 0; k < n; k++) {
+            const double xv = xc[s * XL + k];
+            acc0 = fma(Sq[k * 64 + lane], xv, acc0);
+            acc1 = fma(Sq[k * 64 + lane + 32], xv, acc1);
+        }
+        const int64_t t = t0 + s;
+        if (t < T) {
+            const double accs[2] = {acc0, acc1};
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int i = i0 + lane + 32 * u;
+                if (i < ldx) {
+                    const float v = (i < n) ? (float)accs[u] : 0.f;
+                    xo[t * ldx + i] = tf32 ? round_tf32(v) : v;
+                }
+            }
+        }
+    }
+}
+
 // x_out[t][i] = sum_k S(i,k) (x[t][k] - mean[k]) in FP64, rounded once to FP32
 // (padded channels zero).  Persistent CTAs of 512 threads; S staged in shared
 // memory; a thread computes 4 channels x 4 samples of a 64-sample tile.
@@ -388,8 +663,9 @@ namespace amica {
 // evwork: >= 4 n^2 + 4 n doubles
 cudaError_t launch_preprocess(const float* raw, int64_t T, int n, int do_sphere, double* means,
                               double* cov, double* sphere, double* evwork, double* ldetS_dev,
-                              float* x, int ldx, int tf32, cudaStream_t st) {
-    if (n > 128 || ldx > 128) return cudaErrorInvalidValue;
+                              float* x, int ldx, int tf32, int* err, cudaStream_t st) {
+    if (n > 256 || ldx > 256) return cudaErrorInvalidValue;
+    const bool big = n > 128;
     const int nblk = (int)((T + kChunk - 1) / kChunk);
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
@@ -406,17 +682,50 @@ cudaError_t launch_preprocess(const float* raw, int64_t T, int n, int do_sphere,
     double* V = evwork;
     double* ev = evwork + (size_t)n * n;
     double* var = ev + n;
-    if (do_sphere == 1) {
+    if (do_sphere == 1 && !big) {
         k_cov8<<<ncov, 256, 0, st>>>(raw, T, n, chunk, means, part);
         k_cov_reduce<<<(n * n + 255) / 256, 256, 0, st>>>(part, ncov, n, T, cov);
         const size_t jsmem = sizeof(double) * (size_t)((((n * (n + 1)) / 2 + 1) & ~1) + n * n);
         e = cudaFuncSetAttribute(k_jacobi_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)jsmem);
         if (e != cudaSuccess) { cudaFreeAsync(part, st); return e; }
         k_jacobi_smem<<<1, kJacThreads, jsmem, st>>>(cov, V, ev, n);
+    } else if (do_sphere == 1) {
+        const size_t csmem = sizeof(double) * 2 * kCovRows * 128;
+        e = cudaFuncSetAttribute(k_cov8q, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem);
+        if (e != cudaSuccess) { cudaFreeAsync(part, st); return e; }
+        k_cov8q<<<dim3(ncov, 4), 256, csmem, st>>>(raw, T, n, chunk, means, part);
+        k_cov_reduce<<<(n * n + 255) / 256, 256, 0, st>>>(part, ncov, n, T, cov);
+        // Jacobi state in the (now free) partial buffer: packed triangle, the
+        // stopping-test partials, the barrier counter and the abort flag
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi_grid, kJacThreads, 0);
+        if (e != cudaSuccess || per_sm < 1) { cudaFreeAsync(part, st); return e ? e : cudaErrorInvalidValue; }
+        const int nb = nsm < 64 ? nsm : 64;
+        const size_t np = (size_t)n * (n + 1) / 2;
+        JacGlobal jg;
+        jg.ap = part;
+        jg.part = part + np;
+        jg.count = reinterpret_cast<unsigned*>(part + np + 2 * nb);
+        jg.abort = reinterpret_cast<int*>(part + np + 2 * nb + 1);
+        e = cudaMemsetAsync(part + np + 2 * nb, 0, 2 * sizeof(double), st);
+        if (e != cudaSuccess) { cudaFreeAsync(part, st); return e; }
+        void* args[] = {(void*)&cov, (void*)&V, (void*)&ev, (void*)&n, (void*)&jg, (void*)&err};
+        e = cudaLaunchCooperativeKernel((const void*)k_jacobi_grid, dim3(nb), dim3(kJacThreads), args, 0, st);
+        if (e != cudaSuccess) { cudaFreeAsync(part, st); return e; }
     } else if (do_sphere == 2) {
         k_var<<<n, 256, 0, st>>>(raw, T, n, means, var);
     }
     k_sphere<<<(n * n + 255) / 256, 256, 0, st>>>(V, ev, var, n, do_sphere, sphere, ldetS_dev);
+    if (big) {
+        const size_t smemq = sizeof(double) * (256 * 64 + kSphTileQ * 257);
+        e = cudaFuncSetAttribute(k_apply_sphere_q, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemq);
+        if (e != cudaSuccess) { cudaFreeAsync(part, st); return e; }
+        const int64_t ntq = (T + kSphTileQ - 1) / kSphTileQ;
+        const int gq = (int)(ntq < nsm ? ntq : nsm);
+        k_apply_sphere_q<<<dim3(gq, (ldx + 63) / 64), 512, smemq, st>>>(raw, T, n, means, sphere, x, ldx, tf32);
+        cudaFreeAsync(part, st);
+        return cudaGetLastError();
+    }
     const size_t smem2 = sizeof(double) * (128 * 128 + kSphTile * 129);
     e = cudaFuncSetAttribute(k_apply_sphere8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);
     if (e != cudaSuccess) { cudaFreeAsync(part, st); return e; }

@@ -1,0 +1,110 @@
+"""128 < n <= 256 channels: the channel-split plain E-step (four CTAs per model
+in one cluster), the Gauss-Jordan inverse on a global working copy, and the
+GPU sphering (quadrant covariance, grid-wide Jacobi, sliced sphere apply),
+against the FP64 oracle and numpy.  Above 128 channels the mixed-precision
+request runs the plain FP32 E-step (the tensor-core form holds W in one SM).
+
+Tolerances are those of tests/test_engine_gpu.py (FP32 densities and sums,
+FP64 totals): E-step sums 2e-5 relative, LL 2e-6 nats per sample and channel
+at identical parameters, x5 per iteration along a trajectory; mu_den (see
+compare_stats) through its median and the share of entries off by over 1%.
+"""
+import numpy as np
+import pytest
+
+from cudamica_b200 import synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+STAT_KEYS_TIGHT = ("vs", "cn", "s2", "us", "kn", "ln", "mn", "bd", "rn", "phi")
+
+
+def case(n, T, M, m, seed):
+    d = synth.config2(seed=seed, n=n, T=T, M=M, m=m, block_lo=500, block_hi=1500)
+    xs, means, S, ldetS = O.preprocess(d.x, 1)
+    A0, c0 = synth.norand_init(n, M)
+    return d.x, xs, means, S, ldetS, A0, c0
+
+
+def engine(n, T, M, m, xs, means, S, ldetS, A0, c0, precision=0):
+    from cudamica_b200.engine import Amica
+    eng = Amica(n, T, M, m, precision=precision, update_rho=1)
+    eng.set_sphered(xs, means, S, ldetS)
+    eng.init(A0, c0)
+    return eng
+
+
+def compare_stats(s_gpu, s_orc, n, M, m):
+    a = O.split_stats(s_gpu, n, M, m)
+    b = O.split_stats(s_orc, n, M, m)
+    vsum = float(np.max(b["vs"]))
+    errs = {}
+    for k in STAT_KEYS_TIGHT + ("md",):
+        scale = max(np.max(np.abs(b[k])), vsum if k == "cn" else 0.0)
+        errs[k] = float(np.max(np.abs(a[k] - b[k])) / max(scale, 1e-300))
+    for k in STAT_KEYS_TIGHT:
+        assert errs[k] < 2e-5, (k, errs)
+    # mu_den = rho sum u |y|^(rho-2) (rho <= 2) is carried by the few samples
+    # with y near 0, where the FP32 b moves single entries by tens of percent
+    # (the worst of the n m M entries reached 0.27 here): the test bounds its
+    # typical entry and the share of entries off by more than 1%
+    rel = np.abs(a["md"] - b["md"]) / np.maximum(np.abs(b["md"]), 1e-300)
+    q = np.quantile(rel, [0.5, 0.9, 0.99, 1.0])
+    print("mu_den relative error quantiles 50/90/99/100%:", q)
+    assert q[0] < 1e-4, q
+    assert float(np.mean(rel > 1e-2)) < 0.02, q
+    return errs
+
+
+@pytest.mark.parametrize("n,M,m,precision", [(256, 2, 3, 0), (200, 1, 5, 1), (160, 3, 2, 0)])
+def test_estep_stats_match_oracle(n, M, m, precision):
+    T = 12000
+    x, xs, means, S, ldetS, A0, c0 = case(n, T, M, m, seed=n + M)
+    eng = engine(n, T, M, m, xs, means, S, ldetS, A0, c0, precision)
+    assert eng.kernel == "plain_fp32"
+    orc = O.Oracle(xs, M, m, A0, c0, ldetS, nthreads=8, update_rho=1)
+    orc.prepare()
+    s_orc = orc.estep()
+    s_gpu = eng.estep_stats()
+    assert abs(s_gpu[0] - s_orc[0]) / (n * T) < 2e-6
+    compare_stats(s_gpu, s_orc, n, M, m)
+    # the inverse behind the E-step: W = A^{-1} per model
+    prm = eng.params()
+    for h in range(M):
+        Winv = np.linalg.inv(A0.reshape(M, n, n)[h].T).T   # A stored column-major
+        err = np.max(np.abs(prm["W"][h] - Winv)) / np.max(np.abs(Winv))
+        assert err < 1e-10, (h, err)
+    eng.close()
+
+
+def test_first_iterations_match_oracle():
+    n, T, M, m = 256, 10000, 2, 3
+    x, xs, means, S, ldetS, A0, c0 = case(n, T, M, m, seed=11)
+    eng = engine(n, T, M, m, xs, means, S, ldetS, A0, c0)
+    orc = O.Oracle(xs, M, m, A0, c0, ldetS, nthreads=8, update_rho=1)
+    for it in range(1, 4):
+        out = eng.step()
+        ll_orc = orc.step()
+        assert abs(out.ll - ll_orc) < 2e-6 * 5 ** (it - 1), (it, out.ll, ll_orc)
+    eng.close()
+
+
+@pytest.mark.parametrize("n", [144, 256])
+def test_gpu_preprocess_matches_oracle(n):
+    T = 20000
+    x, xs, means, S, ldetS, A0, c0 = case(n, T, 1, 3, seed=3)
+    from cudamica_b200.engine import Amica
+    eng = Amica(n, T, 1, 3, precision=0)
+    eng.load_data(x)
+    eng.preprocess()
+    eng.init(A0, c0)
+    S2, means2, ld2 = eng.sphere()
+    assert np.max(np.abs(means2 - means)) < 1e-12
+    assert np.max(np.abs(S2 - S)) / np.max(np.abs(S)) < 1e-9
+    assert abs(ld2 - ldetS) < 1e-8
+    ref = engine(n, T, 1, 3, xs, means, S, ldetS, A0, c0)
+    s1, s2 = eng.estep_stats(), ref.estep_stats()
+    assert abs(s1[0] - s2[0]) / (n * T) < 1e-6
+    eng.close()
+    ref.close()
