@@ -84,7 +84,9 @@ int amica_default_cfg(amica_cfg *cfg);
 
 /* Create a context on cfg->device: replaces initializeDevs()
  * (src/device.cu:190-380) and the allocation half of initializeModels()
- * (src/amica.cu:135-556). */
+ * (src/amica.cu:135-556).  Shapes: 2 <= nchannels <= 256, 1 <= nmmodels <= 8,
+ * 1 <= nsdm <= 5 (else AMICA_ERR_UNSUPPORTED).  AMICA_PREC_MIXED runs the
+ * tensor-core E-step up to 128 channels and the plain FP32 E-step above. */
 int amica_create(const amica_cfg *cfg, amica_ctx **out);
 
 /* Release every device and host resource: replaces finalizeModels() /
@@ -196,7 +198,7 @@ int amica_selftest_umma(int mode, int N, int K, const float *A, const float *B, 
  * or a process that forbids device allocations after start-up).  No
  * counterpart in the reference: its EM loop allocates per-block buffers.
  * All pointers are DEVICE memory owned by the caller: x is T x ldx float32
- * sphered data with ldx the channel count padded to 32, 64 or 128 (padding
+ * sphered data with ldx the channel count padded to 32, 64, 128 or 256 (padding
  * channels zero); A (M x n x n), c, alpha, mu, beta, rho, gm as in
  * amica_set_params(); keep (T bytes) may be NULL with nkeep = T; stats
  * receives amica_stats_len(n, M, m) doubles.  Intermediate data lives in a
