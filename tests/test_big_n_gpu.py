@@ -108,3 +108,27 @@ def test_gpu_preprocess_matches_oracle(n):
     assert abs(s1[0] - s2[0]) / (n * T) < 1e-6
     eng.close()
     ref.close()
+
+
+def test_adjoint_matches_float64_autograd_above_128_channels():
+    # The gradient sweep runs the channel-split E-step in gradient mode.  It is
+    # checked at the starting parameters (rho = 1.5): a few EM steps can drive a
+    # rho to its floor of 1, where f' = sign(y) jumps at y = 0 and a sample whose
+    # FP32 and FP64 b straddle 0 moves that channel's mu and W gradients by ~1e-3
+    # of their scale (seen at n = 160 after two steps), in either E-step form.
+    pytest.importorskip("torch")
+    from test_adjoint_gpu import rel_err, torch_reference
+    from cudamica_b200.engine import Amica
+    n, T, M, m = 160, 6000, 2, 3
+    d = synth.config2(seed=7, n=n, T=T, M=M, m=m, block_lo=500, block_hi=1500)
+    xs, means, S, ldetS = O.preprocess(d.x, 1)
+    A0, c0 = synth.norand_init(n, M)
+    eng = Amica(n, T, M, m, precision=0, update_rho=1)
+    eng.set_sphered(xs, means, S, ldetS)
+    eng.init(A0, c0)
+    ll_g, g_g = eng.adjoint()
+    ll_t, g_t, _, _ = torch_reference(eng, xs, ldetS)
+    assert abs(ll_g - ll_t) < 1e-6, (ll_g, ll_t)
+    for k in ("W", "mu", "beta", "rho"):
+        assert rel_err(g_g[k], g_t[k]) < 2e-4, (k, rel_err(g_g[k], g_t[k]))
+    eng.close()
