@@ -331,12 +331,21 @@ def cohort_arm(args):
 
 
 def profile_case(args):
-    """A few E-step launches per form on the first T samples of the workload."""
+    """A few E-step launches per form on the first T samples of the workload
+    (or, with --profile-shape n,M,m, of the large multi-model recipe at that
+    shape: synth.config4, seed 0)."""
     from cudamica_b200.engine import Amica
-    x, A0, c0 = make_data()
     T = args.T
-    for precision in (1, 0):
-        eng = Amica(WORKLOAD["n"], T, WORKLOAD["M"], WORKLOAD["m"], precision=precision, device=0)
+    if args.profile_shape:
+        from cudamica_b200 import synth
+        n, M, m = (int(v) for v in args.profile_shape.split(","))
+        x = synth.config4(seed=0, n=n, T=T, M=M, m=m).x
+        A0, c0 = synth.norand_init(n, M)
+    else:
+        x, A0, c0 = make_data()
+        n, M, m = WORKLOAD["n"], WORKLOAD["M"], WORKLOAD["m"]
+    for precision in ((0,) if n > 128 else (1, 0)):
+        eng = Amica(n, T, M, m, precision=precision, device=0)
         eng.load_data(np.ascontiguousarray(x[:T]))
         eng.preprocess()
         eng.init(A0, c0)
@@ -360,6 +369,8 @@ def main():
                     help="no timing: run a few fused E-step launches of both forms on a "
                          "T-sample slice (for ncu captures)")
     ap.add_argument("--T", type=int, default=WORKLOAD["T"])
+    ap.add_argument("--profile-shape", default="",
+                    help="n,M,m for --profile-case (data: the large multi-model recipe)")
     ap.add_argument("--cohort", action="store_true",
                     help="the cohort workload instead of the single-fit one")
     ap.add_argument("--cohort-subjects", type=int, default=48)
