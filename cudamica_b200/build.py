@@ -31,7 +31,9 @@ SOURCES = ["engine.cu", "mstep.cu", "estep_plain.cu", "estep_tc.cu", "preprocess
 def _compile(src: str, verbose: bool) -> str:
     obj = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
     inp = os.path.join(CSRC, src)
-    deps = [inp, os.path.join(CSRC, "common.cuh"), os.path.join(ROOT, "include", "amica_b200.h")]
+    # every shared header and included kernel body can change any object
+    deps = [inp, os.path.join(ROOT, "include", "amica_b200.h")] + [
+        os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".inc"))]
     if os.path.exists(obj) and all(os.path.getmtime(obj) >= os.path.getmtime(d) for d in deps
                                    if os.path.exists(d)):
         return obj

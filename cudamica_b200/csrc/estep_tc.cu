@@ -382,423 +382,17 @@ __global__ void __launch_bounds__(kThreads, 1)
         // =========================== control warpgroup: TMA + MMA ================
         asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kCtlRegs));
         if (warp == kDensWarps && lane == 0 && ntile_local > 0) {
-            const uint32_t x_off[2] = {Sh::OFF_X0, Sh::OFF_X1};
-            const uint32_t sbase = smem_u32(sm);
-            auto issue_tma = [&](int k) {
-                const int s = k & 1;
-                const int64_t tile = (int64_t)cid + (int64_t)k * a.nclusters;
-                mbar_expect_tx(&bar[BAR_FULL0 + s], Sh::X_BYTES);
-#pragma unroll
-                for (int cb = 0; cb < Sh::KB; cb++)
-                    tma_load_2d(sbase + x_off[s] + cb * kS * 128, &xmap, cb * 32, (int)(tile * kS),
-                                &bar[BAR_FULL0 + s]);
-            };
-            constexpr uint32_t ID1 = idesc_tf32(128, kS, 0, 0);
-            constexpr uint32_t ID2 = idesc_tf32(128, NP, 0, 0);
-            int issued = 0, consumed = 0;
-            issue_tma(0);
-            issued = 1;
-            if (ntile_local > 1) { issue_tma(1); issued = 2; }
-            bool ok = true;
-            for (int k = 0; k < ntile_local && ok; k++) {
-                const int s = k & 1;
-                const uint32_t u = (uint32_t)(k >> 1);
-                // MMA1 for tile k: needs x stage s and a free b buffer
-                ok = mbar_wait(&bar[BAR_FULL0 + s], u & 1, abort_flag, a.err);
-                if (ok) consumed = k + 1;
-                if (ok && k >= 2) ok = mbar_wait(&bar[BAR_BEMPTY0 + s], (u - 1) & 1, abort_flag, a.err);
-                if (!ok) break;
-                tc_fence_after();
-                const uint32_t xb = sbase + x_off[s];
-#pragma unroll
-                for (int kk = 0; kk < NP / 8; kk++) {
-                    const uint32_t koff = (uint32_t)((kk >> 2) * 0) + (uint32_t)((kk & 3) * 32);
-                    const uint64_t ad = sdesc(sbase + Sh::OFF_W + (kk >> 2) * 128 * 128 + koff, 16, 1024);
-                    const uint64_t bd = sdesc(xb + (kk >> 2) * kS * 128 + koff, 16, 1024);
-                    tc_mma_tf32(tmem_b0 + s * kBcol, ad, bd, ID1, kk > 0 ? 1u : 0u);
-                }
-#pragma unroll
-                for (int kk = 0; kk < NP / 8; kk++) {
-                    const uint64_t bd = sdesc(xb + (kk >> 2) * kS * 128 + (uint32_t)((kk & 3) * 32), 16, 1024);
-                    tc_mma_tf32_ta(tmem_b0 + s * kBcol, tmem + kWloCol + (uint32_t)(kk * 8), bd, ID1, 1u);
-                }
-                tc_commit(&bar[BAR_BFULL0 + s]);
-                // MMA2 for tile k-1: needs its G tile
-                if (k >= 1) {
-                    const int kp = k - 1, sp = kp & 1;
-                    ok = mbar_wait(&bar[BAR_GFULL], (uint32_t)(kp & 1), abort_flag, a.err);
-                    if (!ok) break;
-                    tc_fence_after();
-#pragma unroll
-                    for (int kk = 0; kk < kS / 8; kk++) {
-                        const uint64_t ad = sdesc(sbase + Sh::OFF_G + (kk >> 2) * 128 * 128 + (kk & 3) * 32, 16, 1024);
-                        const uint64_t bd = sdesc(sbase + Sh::OFF_BT + (kk >> 2) * 128 * 128 + (kk & 3) * 32, 16, 1024);
-                        tc_mma_tf32(tmem_psi, ad, bd, ID2, (kp > 0 || kk > 0) ? 1u : 0u);
-                    }
-                    tc_commit(&bar[BAR_EMPTY0 + sp]);
-                    tc_commit(&bar[BAR_GEMPTY]);
-                    // stage sp is refilled with tile k+1 once MMA2(k-1) has read it
-                    if (k + 1 < ntile_local) {
-                        ok = mbar_wait(&bar[BAR_EMPTY0 + sp], (uint32_t)((kp >> 1) & 1), abort_flag, a.err);
-                        if (!ok) break;
-                        issue_tma(k + 1);
-                        issued = k + 2;
-                    }
-                }
-            }
-            // MMA2 for the last tile
-            if (ok) {
-                const int kp = ntile_local - 1;
-                ok = mbar_wait(&bar[BAR_GFULL], (uint32_t)(kp & 1), abort_flag, a.err);
-                if (ok) {
-                    tc_fence_after();
-#pragma unroll
-                    for (int kk = 0; kk < kS / 8; kk++) {
-                        const uint64_t ad = sdesc(sbase + Sh::OFF_G + (kk >> 2) * 128 * 128 + (kk & 3) * 32, 16, 1024);
-                        const uint64_t bd = sdesc(sbase + Sh::OFF_BT + (kk >> 2) * 128 * 128 + (kk & 3) * 32, 16, 1024);
-                        tc_mma_tf32(tmem_psi, ad, bd, ID2, (kp > 0 || kk > 0) ? 1u : 0u);
-                    }
-                    tc_commit(&bar[BAR_PSI]);
-                }
-            }
-            // drain: every TMA load this thread issued has landed and every MMA it
-            // issued has completed before the CTA frees tensor memory (bounded)
-            for (int t = consumed; t < issued; t++)
-                mbar_wait(&bar[BAR_FULL0 + (t & 1)], (uint32_t)((t >> 1) & 1), abort_flag, a.err, false,
-                          false);
-            tc_commit(&bar[BAR_DRAIN]);
-            mbar_wait(&bar[BAR_DRAIN], 0u, abort_flag, a.err, false, false);
+            const CUtensorMap* item_map = &xmap;
+            const int64_t item_tile0 = cid, item_stride = a.nclusters;
+#include "tc_control_item.inc"
         }
         __syncwarp();
     } else {
         // =========================== density warps =================================
         asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kDensRegs));
-        const int wg = warp >> 2, q4 = warp & 3;
-        constexpr int npc = NP / R;
-        constexpr int wps = npc / 32;              // warps per sample set
-        const int set = q4 / wps;                  // this warp's sample set
-        const bool lead = (q4 % wps) == 0;         // first warp of its set
-        const int tl = q4 * 32 + lane;             // TMEM lane = row of the G / b tiles
-        const int ch = tl - set * npc;             // channel of this lane
-        const bool ch_ok = ch < n;
-        const uint32_t lane_addr = (uint32_t)(q4 * 32) << 16;
-        // log2|y| of phase 1 is kept in tensor memory for phase 2 when it fits
-        constexpr bool kCacheL2 = kWG * MM <= kL2Chunks;
-        // mixtures (0,1), (2,3) as float2 pairs, an odd last one as a scalar
-        constexpr int NPR = MM / 2;
-        constexpr bool kOdd = (MM & 1) != 0;
-        constexpr int NPRA = NPR > 0 ? NPR : 1;
-        float pr[MM];
-        MixV<float2> P2[NPRA];
-        MixV<float> P1;
-#pragma unroll
-        for (int j = 0; j < MM; j++) {
-            const MixParam q = a.mp[((size_t)h * MM + j) * npc + ch];
-            const float sj = q.s, oj = -q.off;
-            const float cj = q.cl2, rj = q.rho;
-            pr[j] = rj;
-            if (j < 2 * NPR) {
-                float2* f[5] = {&P2[j / 2].s, &P2[j / 2].npo, &P2[j / 2].pc, &P2[j / 2].pr, &P2[j / 2].sr};
-                const float vals[5] = {sj, oj, cj, rj, sj * rj};
-#pragma unroll
-                for (int e = 0; e < 5; e++) {
-                    if (j & 1) f[e]->y = vals[e];
-                    else f[e]->x = vals[e];
-                }
-            } else {
-                P1.s = sj; P1.npo = oj; P1.pc = cj; P1.pr = rj; P1.sr = sj * rj;
-            }
-        }
-        const float wci = a.wc[(size_t)h * npc + ch];
-        float ltc_all[kMaxModels];
-#pragma unroll
-        for (int q = 0; q < kMaxModels; q++) ltc_all[q] = (q < M) ? (float)(a.ltc64[q] - a.ltc64[0]) : 0.f;
-        float* lse_sm = (float*)(sm + Sh::OFF_LSE) + (size_t)wg * kSub * 128 + tl;
-
-        // Per (channel, mixture), with u = v z, p = |y|^rho, r = 1/y:
-        //   A0 = sum u, A1 = sum u p, A2 = sum u p^2, A3 = sum u p log2|y|,
-        //   A4 = sum u p r, A5 = sum u p r^2, A6 = sum u p^2 r^2.
-        // Since f' = rho sign(y)|y|^(rho-1) = rho p r, the reference's sums
-        // (src/kernels.cu:495-827) are: usum = A0, sum u f'^2 = rho^2 A6,
-        // sum u (f' y - 1)^2 = rho^2 A2 - 2 rho A1 + A0, sum u f' = rho A4,
-        // sum u f'/y = rho A5, sum u f' y = rho A1, sum u |y|^rho = A1,
-        // sum u |y|^rho log|y|^rho = rho ln2 A3.  They are formed in FP64 at
-        // each flush.
-        float2 fP[NPRA][7];
-        float fS1[7];
-        float fCn = 0.f, fS2 = 0.f, fGs = 0.f;
-        auto zero_acc = [&]() {
-#pragma unroll
-            for (int k = 0; k < 7; k++) {
-#pragma unroll
-                for (int q = 0; q < NPRA; q++) fP[q][k] = make_float2(0.f, 0.f);
-                fS1[k] = 0.f;
-            }
-            fCn = fS2 = fGs = 0.f;
-        };
-        auto acc_get = [&](int k, int j) -> float {
-            if (j < 2 * NPR) return (j & 1) ? fP[j / 2][k].y : fP[j / 2][k].x;
-            return fS1[k];
-        };
-        zero_acc();
-        double dLL = 0.0, dVs = 0.0;
-        // this thread's partial slot (one per warpgroup and sample set)
-        PartLayout L{n, MM};
-        double* out = a.partial + ((size_t)(cid * ta.ngroups + set * kWG + wg) * M + h) * L.stride();
-        // phi of this set lives in its warpgroup-0 slot
-        double* out0 = a.partial + ((size_t)(cid * ta.ngroups + set * kWG) * M + h) * L.stride();
-        auto flush = [&]() {
-            if (ch_ok) {
-#pragma unroll
-                for (int j = 0; j < MM; j++) {
-                    double us, kn, ln, mn, md, bd, rn;
-                    mix_stats_from_sums(acc_get(0, j), acc_get(1, j), acc_get(2, j), acc_get(3, j),
-                                        acc_get(4, j), acc_get(5, j), acc_get(6, j), pr[j],
-                                        a.grad_mode, a.update_rho, us, kn, ln, mn, md, bd, rn);
-                    const int o = j * n + ch;
-                    red_add_f64(out + L.mix(kUs) + o, us);
-                    red_add_f64(out + L.mix(kKn) + o, kn);
-                    red_add_f64(out + L.mix(kLn) + o, ln);
-                    red_add_f64(out + L.mix(kMn) + o, mn);
-                    red_add_f64(out + L.mix(kMd) + o, md);
-                    red_add_f64(out + L.mix(kBd) + o, bd);
-                    if (a.update_rho) red_add_f64(out + L.mix(kRn) + o, rn);
-                }
-                red_add_f64(out + L.cn() + ch, (double)fCn);
-                red_add_f64(out + L.s2() + ch, (double)fS2);
-                red_add_f64(out + L.gs() + ch, (double)fGs);
-            }
-            zero_acc();
-        };
-        // zero this thread's fields of the slot
-        if (ch_ok) {
-            for (int k = 0; k < 7 * MM; k++) out[L.mix(0) + k * n + ch] = 0.0;
-            out[L.cn() + ch] = 0.0;
-            out[L.s2() + ch] = 0.0;
-            out[L.gs() + ch] = 0.0;
-        }
-        bool ok = true;
-        for (int k = 0; k < ntile_local && ok; k++) {
-            const int s = k & 1;
-            const uint32_t u = (uint32_t)(k >> 1);
-            // packed rows of this warpgroup's slice; lane t < kSub owns row t0 + t,
-            // i.e. sample (t0 + t) R + set
-            const int64_t t0 = ((int64_t)cid + (int64_t)k * a.nclusters) * kS + wg * kSub;
-            // this tile's keep flags, fetched now and used after the exchange
-            const int64_t tk = (t0 + (lane < kSub ? lane : kSub - 1)) * R + set;
-            const bool in_range = tk < a.T;
-            const bool kept = in_range && (a.keep == nullptr || a.keep[tk]);
-            const int par = k & 1;
-            uint64_t* ltbar = &bar[BAR_LT0 + par * kWG + wg];
-            // this tile's exchange: 4 warps x kSub samples x M models of 4 bytes
-            if (q4 == 0 && lane == 0) mbar_expect_tx(ltbar, (uint32_t)(4 * kSub * M * 4));
-            ok = mbar_wait(&bar[BAR_BFULL0 + s], u & 1, abort_flag, a.err);
-            if (!ok) break;
-            tc_fence_after();
-            const uint32_t bcol = tmem_b0 + lane_addr + (uint32_t)(s * kBcol + wg * kSub);
-
-            // ---- phase 1: per-sample log-sum-exp over mixtures (log2 units), 4 samples at a
-            // time; the channel sum per sample is a 4-value transposed butterfly over the
-            // warp's 32 lanes, after which lane 8q holds the warp's sum for sample 4g+q
-            uint32_t bnext[4];
-            tmem_ld4_nowait(bcol, bnext);
-#pragma unroll 1
-            for (int g4 = 0; g4 < kSub / 4; g4++) {
-                float bx[4], v[4], l2c[MM][4];
-                tmem_wait_ld(bnext);
-#pragma unroll
-                for (int r = 0; r < 4; r++) bx[r] = __uint_as_float(bnext[r]);
-                if (g4 + 1 < kSub / 4) tmem_ld4_nowait(bcol + (uint32_t)(g4 * 4 + 4), bnext);
-#pragma unroll
-                for (int r = 0; r < 4; r++) {
-                    float q[MM];
-#pragma unroll
-                    for (int qq = 0; qq < NPR; qq++) {
-                        float2 L2;
-                        const float2 q2 = dens_q(P2[qq], bx[r], L2);
-                        q[2 * qq] = q2.x; q[2 * qq + 1] = q2.y;
-                        l2c[2 * qq][r] = L2.x; l2c[2 * qq + 1][r] = L2.y;
-                    }
-                    if constexpr (kOdd) {
-                        float L2;
-                        q[MM - 1] = dens_q(P1, bx[r], L2);
-                        l2c[MM - 1][r] = L2;
-                    }
-                    const float lse = lse2<MM>(q);
-                    lse_sm[(g4 * 4 + r) * 128] = lse;
-                    v[r] = ch_ok ? lse : 0.f;
-                }
-                if constexpr (kCacheL2) {
-#pragma unroll
-                    for (int j = 0; j < MM; j++)
-                        tmem_st4_nowait(tmem + lane_addr + l2_chunk_col(wg * MM + j) + (uint32_t)(g4 * 4),
-                                        l2c[j]);
-                }
-                {
-                    const bool up16 = (lane & 16) != 0;
-                    const float s0 = up16 ? v[0] : v[2], s1 = up16 ? v[1] : v[3];
-                    const float k0 = up16 ? v[2] : v[0], k1 = up16 ? v[3] : v[1];
-                    v[0] = k0 + __shfl_xor_sync(0xffffffffu, s0, 16);
-                    v[1] = k1 + __shfl_xor_sync(0xffffffffu, s1, 16);
-                    const bool up8 = (lane & 8) != 0;
-                    const float s2 = up8 ? v[0] : v[1], k2 = up8 ? v[1] : v[0];
-                    float w = k2 + __shfl_xor_sync(0xffffffffu, s2, 8);
-                    w += __shfl_xor_sync(0xffffffffu, w, 4);
-                    w += __shfl_xor_sync(0xffffffffu, w, 2);
-                    w += __shfl_xor_sync(0xffffffffu, w, 1);
-                    // lane bits (4,3) select the sample: 2*bit4 + bit3; the warp's sum
-                    // goes to every model's CTA
-                    if ((lane & 7) == 0) {
-                        const int t = wg * kSub + g4 * 4 + ((lane >> 4) & 1) * 2 + ((lane >> 3) & 1);
-                        const uint32_t sl = smem_u32(slot + ((par * kMaxModels + h) * 4 + q4) * kS + t);
-                        const uint32_t lb = smem_u32(ltbar);
-                        for (int q = 0; q < M; q++) st_async_f32(mapa(sl, (uint32_t)q), w, mapa(lb, (uint32_t)q));
-                    }
-                }
-            }
-            if constexpr (kCacheL2) tmem_wait_st();
-            ok = mbar_wait(ltbar, u & 1, abort_flag, a.err, true);
-            if (!ok) break;
-            // ---- P(t), v_h(t): lanes < kSub of every warp, one sample each
-            float vme = 0.f;
-            {
-                const int t = lane < kSub ? lane : kSub - 1;
-                float Lq[kMaxModels];
-                float lmax = -INFINITY;
-#pragma unroll
-                for (int q = 0; q < kMaxModels; q++) {
-                    if (q < M) {
-                        const float* sq = slot + (par * kMaxModels + q) * 4 * kS + wg * kSub + t;
-                        // this set's warps, in order
-                        float sw = sq[set * wps * kS];
-#pragma unroll
-                        for (int w = 1; w < wps; w++) sw += sq[(set * wps + w) * kS];
-                        Lq[q] = ltc_all[q] + kLn2 * sw;
-                        lmax = fmaxf(lmax, Lq[q]);
-                    }
-                }
-                float se = 0.f;
-#pragma unroll
-                for (int q = 0; q < kMaxModels; q++)
-                    if (q < M) se += ptx_ex2((Lq[q] - lmax) * kLog2e);
-                const float P = lmax + kLn2 * ptx_lg2(se);
-                float Lmine = 0.f;
-#pragma unroll
-                for (int q = 0; q < kMaxModels; q++)
-                    if (q == h) Lmine = Lq[q];
-                const float vh = ptx_ex2((Lmine - P) * kLog2e);
-                const int64_t tg = tk;
-                const bool valid = kept;
-                vme = valid ? vh : 0.f;
-                if (lead && lane < kSub) {
-                    if (valid) {
-                        dVs += (double)vh;
-                        if (h == 0) dLL += (double)P;
-                    }
-                    if (in_range) {
-                        if (a.Lt_out) a.Lt_out[(size_t)h * a.T + tg] = Lmine;
-                        if (a.P_out && h == 0) a.P_out[tg] = P;
-                    }
-                }
-            }
-            // ---- phase 2 (G tile is free once MMA2 of the previous tile has run)
-            if (k >= 1) {
-                ok = mbar_wait(&bar[BAR_GEMPTY], (uint32_t)((k - 1) & 1), abort_flag, a.err);
-                if (!ok) break;
-            }
-#pragma unroll 1
-            for (int g4 = 0; g4 < kSub / 4; g4++) {
-                float bx[4], gq[4], bq[4];
-                uint32_t l2r[MM][4];
-                {
-                    uint32_t br[4];
-                    tmem_ld4_nowait(bcol + (uint32_t)(g4 * 4), br);
-                    if constexpr (kCacheL2) {
-#pragma unroll
-                        for (int j = 0; j < MM; j++)
-                            tmem_ld4_nowait(tmem + lane_addr + l2_chunk_col(wg * MM + j) + (uint32_t)(g4 * 4),
-                                            l2r[j]);
-                    }
-                    tmem_wait_ld(br);
-                    if constexpr (kCacheL2) {
-#pragma unroll
-                        for (int j = 0; j < MM; j++) tmem_wait_ld(l2r[j]);
-                    }
-#pragma unroll
-                    for (int r = 0; r < 4; r++) bx[r] = __uint_as_float(br[r]);
-                }
-#pragma unroll
-                for (int r = 0; r < 4; r++) {
-                    const float v = __shfl_sync(0xffffffffu, vme, g4 * 4 + r);
-                    const float lse = lse_sm[(g4 * 4 + r) * 128];
-                    float2 g2 = make_float2(0.f, 0.f);
-                    float g1 = 0.f;
-#pragma unroll
-                    for (int qq = 0; qq < NPR; qq++) {
-                        float2 L2 = make_float2(0.f, 0.f);
-                        if constexpr (kCacheL2)
-                            L2 = make_float2(__uint_as_float(l2r[2 * qq][r]), __uint_as_float(l2r[2 * qq + 1][r]));
-                        dens_acc<float2, kCacheL2>(P2[qq], bx[r], L2, -lse, v, fP[qq], g2);
-                    }
-                    if constexpr (kOdd) {
-                        float L2 = 0.f;
-                        if constexpr (kCacheL2) L2 = __uint_as_float(l2r[MM - 1][r]);
-                        dens_acc<float, kCacheL2>(P1, bx[r], L2, -lse, v, fS1, g1);
-                    }
-                    float g = (g2.x + g2.y) + g1;
-                    const float bb = bx[r] - wci;
-                    fCn = fmaf(v, bb, fCn);
-                    fS2 = fmaf(v * bb, bb, fS2);
-                    g = ch_ok ? g : 0.f;
-                    fGs += g;
-                    gq[r] = tf32_rna(g);
-                    bq[r] = ch_ok ? tf32_rna(bb) : 0.f;
-                }
-                const uint32_t goff = sw128_off(tl, wg * kSub + g4 * 4, 128);
-                *reinterpret_cast<float4*>((uint8_t*)Gsm + goff) = make_float4(gq[0], gq[1], gq[2], gq[3]);
-                *reinterpret_cast<float4*>(sm + Sh::OFF_BT + goff) = make_float4(bq[0], bq[1], bq[2], bq[3]);
-            }
-            // b buffer s fully consumed: release it to MMA1 of tile k+2
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&bar[BAR_BEMPTY0 + s]);
-            fence_proxy_async();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&bar[BAR_GFULL]);
-            if ((k + 1) % kFlush == 0) flush();
-        }
-        flush();
-        // vsum / LL of this warpgroup and set (its first warp accumulated them)
-        if (lead) {
-            double a1 = dLL, a2 = dVs;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-                a2 += __shfl_xor_sync(0xffffffffu, a2, o);
-            }
-            if (lane == 0) {
-                out[0] = a1;
-                out[1] = a2;
-            }
-        }
-        // ---- Psi_h out of tensor memory: the diagonal block of this set (columns
-        // [set*npc, set*npc + npc)), in 16-column chunks dealt round-robin to the
-        // warpgroups; the R blocks are summed by the slot reduction
-        if (ok && ntile_local > 0) ok = mbar_wait(&bar[BAR_PSI], 0u, abort_flag, a.err);
-        if (ok && ntile_local > 0) {
-            tc_fence_after();
-#pragma unroll
-            for (int c0 = 0; c0 < npc; c0 += 16) {
-                if ((c0 / 16) % kWG != wg) continue;
-                float v[16];
-                tmem_ld16(tmem_psi + lane_addr + (uint32_t)(set * npc + c0), v);
-#pragma unroll
-                for (int q = 0; q < 16; q++) {
-                    const int kcol = c0 + q;
-                    if (ch_ok && kcol < n) out0[L.psi() + (size_t)kcol * n + ch] = (double)v[q];
-                }
-            }
-        }
+        const int64_t item_tile0 = cid, item_stride = a.nclusters;
+        const int item_slot = cid, item_ngroups = ta.ngroups;
+#include "tc_density_item.inc"
     }
     tc_fence_before();
     cluster.sync();
