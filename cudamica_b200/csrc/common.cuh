@@ -93,6 +93,19 @@ struct EStepArgs {
     int grad_mode;           // 1: beta-denominator slot holds sum u*f'*y for every rho (adjoint)
 };
 
+// The cohort E-step (one persistent launch over many single-model fits): a
+// subject's arguments and lane packing, and a run of its tiles.
+struct TcCohortSub {
+    EStepArgs a;   // the subject's E-step arguments (M = 1)
+    int R;         // lane packing of its channel count (128 / padded channels)
+};
+struct TcCohortItem {
+    int sub;       // subject
+    int slot;      // partial-slot group in the subject's buffer
+    int64_t tile0; // first tile
+    int ntiles;    // consecutive tiles
+};
+
 // Device buffers and host-side settings of the FP64 M-step kernels.
 struct MStepBuffers {
     double *A, *Anew, *c, *alpha, *mu, *beta, *rho, *gm, *W, *ldet, *ltc64;

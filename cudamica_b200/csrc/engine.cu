@@ -11,6 +11,7 @@
 // per iteration.  This replaces runamica()'s iteration body
 // (src/amica.cu:820-2541), which synchronised with the host ~T/block_size
 // times per iteration.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -35,6 +36,10 @@ int tc_max_clusters(int n, int m, int M);
 int tc_tile_samples(int n);
 int tc_partial_groups(int n);
 int tc_psi_step();
+int tc_cohort_encode_map(const EStepArgs& a, void* map);
+int tc_cohort_ctas();
+cudaError_t launch_estep_tc_cohort(const TcCohortSub* subs, const void* maps, const TcCohortItem* items,
+                                   const int* item_off, int nctas, int m, cudaStream_t st);
 int tc_selftest(int mode, int N, int K, const float* hA, const float* hB, float* hD, int* derr);
 cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStream_t st);
 // preprocess.cu
@@ -97,6 +102,20 @@ struct amica_ctx {
     cudaGraphExec_t graph = nullptr;
     int64_t pending = -1;         // iterations enqueued by amica_run_async, -1 if none
     int64_t pending_it0 = 0;
+};
+
+struct amica_cohort {
+    std::vector<amica_ctx*> subs;
+    int dev = 0, m = 0, nctas = 0, nitems = 0;
+    cudaStream_t st = nullptr;                    // the cohort E-step's stream
+    cudaEvent_t fork = nullptr, mid = nullptr, ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> evs;                 // per subject: prep done, M-step done
+    std::vector<int> nslots;                      // per subject: partial slots its items fill
+    TcCohortSub* d_subs = nullptr;
+    unsigned char* d_maps = nullptr;              // one CUtensorMap (128 bytes) per subject
+    TcCohortItem* d_items = nullptr;
+    int* d_off = nullptr;                         // items of CTA c: [d_off[c], d_off[c + 1])
+    cudaGraphExec_t graph = nullptr;
 };
 
 namespace {
@@ -899,6 +918,190 @@ int amica_time_estep(amica_ctx* c, int64_t reps, double* ms_per_launch, int64_t*
     *ms_per_launch = (double)ms / (double)reps;
     if (launches) *launches = reps + 2;
     return AMICA_OK;
+}
+
+// ---------------------------------------------------------------- cohort
+// Several single-model fits (the same m) advanced together: per iteration, each
+// subject's inverse/derive on its own stream, ONE persistent tensor-core E-step
+// over all subjects' tiles (estep_tc_cohort_kernel), then each subject's
+// reduction and M-step on its own stream -- captured as one CUDA graph.  The
+// tiles of all subjects are dealt to the CTAs (one per SM) as contiguous
+// ranges of the concatenated tile list, so every CTA gets the same number of
+// tiles; a range that crosses subjects becomes one work item per subject.
+int amica_cohort_create(amica_ctx* const* ctxs, int64_t nsub, amica_cohort** out) {
+    if (!ctxs || nsub < 1 || !out) return AMICA_ERR_INVALIDPARAM;
+    *out = nullptr;
+    const amica_ctx* c0 = ctxs[0];
+    if (!c0) return AMICA_ERR_INVALIDPARAM;
+    for (int64_t s = 0; s < nsub; s++) {
+        const amica_ctx* c = ctxs[s];
+        if (!c || c->dev != c0->dev || c->m != c0->m) return AMICA_ERR_INVALIDPARAM;
+        if (!c->use_tc || c->M != 1) return AMICA_ERR_UNSUPPORTED;
+    }
+    CK(cudaSetDevice(c0->dev));
+    amica_cohort* co = new amica_cohort();
+    co->subs.assign(ctxs, ctxs + nsub);
+    co->dev = c0->dev;
+    co->m = c0->m;
+    co->nctas = tc_cohort_ctas();
+    // deal the concatenated tiles to the CTAs
+    std::vector<int64_t> first(nsub + 1, 0);
+    for (int64_t s = 0; s < nsub; s++) first[s + 1] = first[s] + co->subs[s]->ntiles;
+    const int64_t N = first[nsub];
+    std::vector<TcCohortItem> items;
+    std::vector<int> off(co->nctas + 1, 0), nitem(nsub, 0);
+    for (int cta = 0; cta < co->nctas; cta++) {
+        const int64_t a0 = N * cta / co->nctas, a1 = N * (cta + 1) / co->nctas;
+        int64_t t = a0;
+        int s = 0;
+        while (s < nsub && first[s + 1] <= t) s++;
+        while (t < a1 && s < nsub) {
+            const int64_t e = std::min(a1, first[s + 1]);
+            TcCohortItem it;
+            it.sub = s;
+            it.slot = nitem[s]++;
+            it.tile0 = t - first[s];
+            it.ntiles = (int)(e - t);
+            items.push_back(it);
+            t = e;
+            s++;
+        }
+        off[cta + 1] = (int)items.size();
+    }
+    std::vector<TcCohortSub> subs(nsub);
+    std::vector<unsigned char> maps((size_t)nsub * 128);
+    for (int64_t s = 0; s < nsub; s++) {
+        amica_ctx* c = co->subs[s];
+        if (nitem[s] > c->nclusters_cap) { delete co; return AMICA_ERR_UNSUPPORTED; }
+        subs[s].a = estep_args(c);
+        subs[s].R = 128 / c->NP;
+        if (tc_cohort_encode_map(subs[s].a, maps.data() + (size_t)s * 128) != 0) {
+            delete co;
+            return AMICA_ERR_CUDA;
+        }
+        co->nslots.push_back(nitem[s] * tc_partial_groups(c->n));
+    }
+    co->nitems = (int)items.size();
+    int r = AMICA_OK;
+#define COAL(p, cnt) if ((r = dalloc(&(p), (cnt))) != AMICA_OK) { amica_cohort_destroy(co); return r; }
+    COAL(co->d_subs, (size_t)nsub);
+    COAL(co->d_maps, (size_t)nsub * 128);
+    COAL(co->d_items, items.size() ? items.size() : 1);
+    COAL(co->d_off, (size_t)co->nctas + 1);
+#undef COAL
+    CK(cudaMemcpy(co->d_subs, subs.data(), sizeof(TcCohortSub) * nsub, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(co->d_maps, maps.data(), maps.size(), cudaMemcpyHostToDevice));
+    if (!items.empty())
+        CK(cudaMemcpy(co->d_items, items.data(), sizeof(TcCohortItem) * items.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(co->d_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
+    CK(cudaStreamCreateWithFlags(&co->st, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&co->fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&co->mid, cudaEventDisableTiming));
+    CK(cudaEventCreate(&co->ev0));
+    CK(cudaEventCreate(&co->ev1));
+    co->evs.resize(2 * nsub);
+    for (auto& e : co->evs) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    *out = co;
+    return AMICA_OK;
+}
+
+int amica_cohort_destroy(amica_cohort* co) {
+    if (!co) return AMICA_OK;
+    cudaSetDevice(co->dev);
+    if (co->st) cudaStreamSynchronize(co->st);
+    if (co->graph) cudaGraphExecDestroy(co->graph);
+    cudaFree(co->d_subs); cudaFree(co->d_maps); cudaFree(co->d_items); cudaFree(co->d_off);
+    for (auto e : co->evs) if (e) cudaEventDestroy(e);
+    for (auto e : {co->fork, co->mid, co->ev0, co->ev1}) if (e) cudaEventDestroy(e);
+    if (co->st) cudaStreamDestroy(co->st);
+    delete co;
+    return AMICA_OK;
+}
+
+static int cohort_capture(amica_cohort* co) {
+    const int ns = (int)co->subs.size();
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(co->st, cudaStreamCaptureModeThreadLocal));
+    auto step = [&]() -> int {
+        CK(cudaEventRecord(co->fork, co->st));
+        for (int s = 0; s < ns; s++) {
+            amica_ctx* c = co->subs[s];
+            CK(cudaStreamWaitEvent(c->st, co->fork, 0));
+            CK(launch_prep(c->b, c->hc, c->st));
+            CK(cudaEventRecord(co->evs[2 * s], c->st));
+            CK(cudaStreamWaitEvent(co->st, co->evs[2 * s], 0));
+        }
+        CK(launch_estep_tc_cohort(co->d_subs, co->d_maps, co->d_items, co->d_off, co->nctas, co->m, co->st));
+        CK(cudaEventRecord(co->mid, co->st));
+        for (int s = 0; s < ns; s++) {
+            amica_ctx* c = co->subs[s];
+            CK(cudaStreamWaitEvent(c->st, co->mid, 0));
+            CK(launch_reduce_finalize(c->b, c->hc, co->nslots[s], c->st));
+            CK(launch_mstep(c->b, c->hc, c->d_P, c->d_keep, c->T, c->st));
+            CK(cudaEventRecord(co->evs[2 * s + 1], c->st));
+            CK(cudaStreamWaitEvent(co->st, co->evs[2 * s + 1], 0));
+        }
+        return AMICA_OK;
+    };
+    const int r = step();
+    cudaError_t ce = cudaStreamEndCapture(co->st, &g);
+    if (r != AMICA_OK) return r;
+    CK(ce);
+    CK(cudaGraphInstantiate(&co->graph, g, 0));
+    CK(cudaGraphDestroy(g));
+    return AMICA_OK;
+}
+
+int amica_cohort_run(amica_cohort* co, int64_t iters, amica_iter_out* hist, double* ms_per_iter) {
+    if (!co || iters < 0) return AMICA_ERR_INVALIDPARAM;
+    CK(cudaSetDevice(co->dev));
+    const int ns = (int)co->subs.size();
+    std::vector<int64_t> it0(ns);
+    for (int s = 0; s < ns; s++) {
+        amica_ctx* c = co->subs[s];
+        if (!c->have_x || !c->have_init) return AMICA_ERR_STATE;
+        if (c->pending >= 0) return AMICA_ERR_STATE;
+        CK(cudaMemcpyAsync(c->h_ctrl, c->b.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        it0[s] = c->h_ctrl->iter;
+        if (it0[s] + iters > c->b.hist_cap) return AMICA_ERR_INVALIDPARAM;
+    }
+    if (!co->graph) TRY(cohort_capture(co));
+    for (int s = 0; s < ns; s++) {
+        amica_ctx* c = co->subs[s];
+        TRY(snapshot_params(c, false));
+        CK(cudaEventRecord(co->evs[2 * s], c->st));
+        CK(cudaStreamWaitEvent(co->st, co->evs[2 * s], 0));
+    }
+    CK(cudaEventRecord(co->ev0, co->st));
+    for (int64_t k = 0; k < iters; k++) CK(cudaGraphLaunch(co->graph, co->st));
+    CK(cudaEventRecord(co->ev1, co->st));
+    CK(cudaStreamSynchronize(co->st));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, co->ev0, co->ev1));
+    if (ms_per_iter) *ms_per_iter = iters ? (double)ms / (double)iters : 0.0;
+    int first_err = AMICA_OK;
+    for (int s = 0; s < ns; s++) {
+        amica_ctx* c = co->subs[s];
+        c->have_estep = c->have_estep || iters > 0;
+        int e = check_device_error(c);
+        CK(cudaMemcpy(c->h_ctrl, c->b.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+        std::vector<IterRec> recs(iters);
+        if (iters > 0)
+            CK(cudaMemcpy(recs.data(), c->b.hist + it0[s], sizeof(IterRec) * iters, cudaMemcpyDeviceToHost));
+        for (int64_t k = 0; k < iters; k++) {
+            if (e == AMICA_OK && !std::isfinite(recs[k].ll)) e = AMICA_ERR_NUMERIC;
+            c->hist.push_back(recs[k]);
+            print_iter(c, recs[k]);
+            if (hist) fill_out(recs[k], *c->h_ctrl, iters ? ms / iters : 0.0, &hist[(size_t)s * iters + k]);
+        }
+        if (e == AMICA_ERR_NUMERIC) {
+            snapshot_params(c, true);
+            cudaStreamSynchronize(c->st);
+        }
+        if (first_err == AMICA_OK) first_err = e;
+    }
+    return first_err;
 }
 
 int amica_get_sphere(amica_ctx* c, double* sphere, double* means, double* ldetS) {

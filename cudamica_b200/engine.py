@@ -42,7 +42,8 @@ EXPORTED = (
     "amica_write_outputs", "amica_status_string", "amica_kernel_name", "amica_get_p_relative",
     "amica_last_cuda_error", "amica_set_iter_state", "amica_get_sphere", "amica_time_estep",
     "amica_launches_per_iteration", "amica_selftest_umma", "amica_estep_stats_noalloc",
-    "amica_run_async", "amica_run_wait", "amica_set_grid")
+    "amica_run_async", "amica_run_wait", "amica_set_grid", "amica_cohort_create",
+    "amica_cohort_run", "amica_cohort_destroy")
 
 
 class Cfg(C.Structure):
@@ -91,6 +92,9 @@ def lib():
         L.amica_run_async.argtypes = [vp, _i64]
         L.amica_set_grid.argtypes = [vp, _i64, C.POINTER(_i64)]
         L.amica_run_wait.argtypes = [vp, C.POINTER(IterOut)]
+        L.amica_cohort_create.argtypes = [C.POINTER(vp), _i64, C.POINTER(vp)]
+        L.amica_cohort_run.argtypes = [vp, _i64, C.POINTER(IterOut), C.POINTER(_dbl)]
+        L.amica_cohort_destroy.argtypes = [vp]
         L.amica_get_params.argtypes = [vp] + [_pd] * 8
         L.amica_set_params.argtypes = [vp] + [_pd] * 7
         L.amica_estep_stats.argtypes = [vp, _pd]
@@ -328,3 +332,37 @@ class Amica:
     def write_outputs(self, **paths) -> None:
         p = Paths(**{k: (v.encode() if v else None) for k, v in paths.items()})
         _chk(lib().amica_write_outputs(self._ctx, C.byref(p)), "amica_write_outputs")
+
+
+class PersistentCohort:
+    """Single-model fits (mixed form, same m) advanced together with one
+    persistent E-step launch per iteration over all their sample tiles
+    (amica_cohort_*).  The engines stay usable on their own; this object does
+    not own them."""
+
+    def __init__(self, engines):
+        self.engines = list(engines)
+        arr = (C.c_void_p * len(self.engines))(*[e._ctx for e in self.engines])
+        h = C.c_void_p()
+        _chk(lib().amica_cohort_create(arr, len(self.engines), C.byref(h)), "amica_cohort_create")
+        self._h = h
+
+    def run(self, iters: int):
+        """`iters` iterations of every subject: (records per subject, ms per
+        cohort iteration on the device)."""
+        S = len(self.engines)
+        outs = (IterOut * max(S * iters, 1))()
+        ms = _dbl()
+        _chk(lib().amica_cohort_run(self._h, iters, outs, C.byref(ms)), "amica_cohort_run")
+        return [[outs[s * iters + k] for k in range(iters)] for s in range(S)], float(ms.value)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().amica_cohort_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

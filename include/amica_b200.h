@@ -230,6 +230,27 @@ int amica_run_async(amica_ctx *ctx, int64_t iters);
 int amica_set_grid(amica_ctx *ctx, int64_t max_clusters, int64_t *nclusters);
 int amica_run_wait(amica_ctx *ctx, amica_iter_out *hist);
 
+/* A cohort: several single-model fits (nmmodels = 1, the same nsdm, the mixed
+ * form, up to 128 channels each, with their own channel counts and lengths)
+ * advanced together with ONE persistent tensor-core E-step launch per
+ * iteration over all subjects' sample tiles (a work list of (subject, tile
+ * range) items dealt evenly to one CTA per SM), each subject's inverse and
+ * M-step running on its own stream around it; an iteration of the whole
+ * cohort is one CUDA graph.  The subjects stay ordinary contexts (parameters,
+ * outputs and history through the per-context calls).  No counterpart in the
+ * reference (one fit per process).
+ * amica_cohort_create: the contexts must be created, and before
+ * amica_cohort_run also sphered and initialised; AMICA_ERR_UNSUPPORTED for
+ * M > 1 or the plain form.  The cohort does not own the contexts.
+ * amica_cohort_run: `iters` iterations of every subject; hist (may be NULL)
+ * receives nsubjects x iters records, subject-major; *ms_per_iter (may be NULL)
+ * the device time of one cohort iteration.  Returns the first subject's error
+ * (each subject rolls back to its parameters before the call on NaN/Inf). */
+typedef struct amica_cohort amica_cohort;
+int amica_cohort_create(amica_ctx *const *subjects, int64_t nsubjects, amica_cohort **out);
+int amica_cohort_run(amica_cohort *cohort, int64_t iters, amica_iter_out *hist, double *ms_per_iter);
+int amica_cohort_destroy(amica_cohort *cohort);
+
 /* Last CUDA runtime error code seen by any call (0 = none). */
 int amica_last_cuda_error(void);
 
