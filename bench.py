@@ -493,7 +493,12 @@ def main():
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_port(x, A0, c0)
     if not args.no_e2e:
-        e2e = e2e_run(x, A0, c0, device, args.steps)
+        # three whole fits, the median reported: a single wall-clock run on a
+        # shared host occasionally lands several times slower than the others
+        runs = [e2e_run(x, A0, c0, device, args.steps) for _ in range(3)]
+        e2e = dict(sorted(runs, key=lambda r: r["value"])[1])
+        e2e["runs"] = [r["value"] for r in runs]
+        e2e["scope"] += ", median of 3 fits"
         if pg:
             e2e["value"] = reduce_over_ranks([e2e["value"]], pg, "min")[0] * ws
         out["e2e"] = e2e
