@@ -195,17 +195,22 @@ def cpu_baseline_port(x, A0, c0, sample_T: int = 100_000):
                       f"({dt:.2f} s), scaled x{scale:g}"}
 
 
-def e2e_run(x, A0, c0, device, steps):
+def pinned_copy(x):
+    """The raw data in page-locked host memory (torch is used only as the
+    allocator), as a user holding the recording for the fit would keep it."""
+    import torch
+    pin = torch.empty(x.shape, dtype=torch.float32, pin_memory=True)
+    pin.numpy()[...] = x
+    return pin
+
+
+def e2e_run(pin, A0, c0, device, steps):
     """Whole fit through the public API from pinned host memory: H2D load,
     GPU sphering, init, `steps` iterations, D2H of the parameters."""
-    import torch
     from cudamica_b200.engine import Amica
     n, T = WORKLOAD["n"], WORKLOAD["T"]
-    # pinned host buffer for the raw data (torch is used only as the allocator)
-    pin = torch.empty((T, n), dtype=torch.float32, pin_memory=True)
     buf = pin.numpy()
-    buf[...] = x
-    nbytes = x.nbytes
+    nbytes = buf.nbytes
     pinned = pin.is_pinned()
     eng = Amica(n, T, WORKLOAD["M"], WORKLOAD["m"], precision=1, device=device, maxiter=4000)
     t0 = time.perf_counter()
@@ -216,7 +221,6 @@ def e2e_run(x, A0, c0, device, steps):
     prm = eng.params()
     dt = time.perf_counter() - t0
     eng.close()
-    del pin
     d2h = sum(v.nbytes for v in prm.values()) + steps * 64
     return {"value": steps / dt, "unit": "iters/s", "h2d_bytes_per_step": nbytes / steps,
             "d2h_bytes_per_step": d2h / steps, "pinned_host": bool(pinned),
@@ -493,12 +497,15 @@ def main():
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_port(x, A0, c0)
     if not args.no_e2e:
-        # three whole fits, the median reported: a single wall-clock run on a
-        # shared host occasionally lands several times slower than the others
-        runs = [e2e_run(x, A0, c0, device, args.steps) for _ in range(3)]
+        # one untimed fit (first-launch costs), then three whole fits from the
+        # same pinned buffer, the median reported
+        pin = pinned_copy(x)
+        e2e_run(pin, A0, c0, device, args.warmup)
+        runs = [e2e_run(pin, A0, c0, device, args.steps) for _ in range(3)]
+        del pin
         e2e = dict(sorted(runs, key=lambda r: r["value"])[1])
         e2e["runs"] = [r["value"] for r in runs]
-        e2e["scope"] += ", median of 3 fits"
+        e2e["scope"] += ", median of 3 fits after one untimed fit"
         if pg:
             e2e["value"] = reduce_over_ranks([e2e["value"]], pg, "min")[0] * ws
         out["e2e"] = e2e

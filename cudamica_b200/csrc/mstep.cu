@@ -39,32 +39,87 @@ __device__ double block_sum(double v, double* sh) {
 // the LU log-determinant (src/amica.cu:27-127, :864-924).
 //
 // Gauss-Jordan elimination with partial pivoting and no row interchanges: the
-// pivot of column k is the not yet used row p_k with the largest |a(p_k, k)|
-// (lowest row on ties).  Eliminating in place turns column k of the working
-// matrix into column p_k of P.A^{-1}, so at the end W(j, p_k) = a(p_j, k).
-// Thread (g, c) = (tid / 128, tid % 128) keeps a(g + 4 i, c), i < 32, in
-// registers.  A pivot step costs two barriers: the owners of column k publish it
-// with their argmax candidates, then the pivot row is published.  Row p is
-// reached in the register array through a switch on the (uniform) index p / 4.
+// pivot of column k is a not yet used row p_k of (nearly) largest |a(p_k, k)|.
+// Sweeping (p_k, k) in place,
+//   a(p, k) <- 1 / a(p, k),   a(p, j) <- a(p, j) / a(p, k),
+//   a(i, k) <- -a(i, k) / a(p, k),   a(i, j) <- a(i, j) - a(i, k) a(p, j) / a(p, k),
+// turns column k into column p_k of P.A^{-1}, so at the end W(j, p_k) = a(p_j, k).
+//
+// Columns are swept in panels of 16.  Warps 0-1 sweep a panel's columns alone
+// (thread r holds rows r and r + 64 of the panel in registers): the pivot of
+// column k only depends on column k as updated by the earlier pivots, and those
+// updates only read the pivot rows' panel entries.  The pivot key of a row is
+// the high word of |a| with its low 7 bits replaced by 127 - row (so the pivot
+// is within 2^-13 of the column's largest |a|, lowest row on ties); each warp's
+// best row publishes its panel row and its reciprocal (every row forms the
+// reciprocal of its candidate while the warp max runs), and after one 64-thread
+// barrier every thread takes the larger key, updates the next column first and
+// starts the next search before the rest of its rows.
+//
+// Sweeping a panel's pivots (P, K) one after another is, on the other columns
+// C, the block sweep
+//   a(i, C) <- [i not in P] a(i, C) + sum_t X(i, t) a_old(p_t, C),
+// X being the swept panel: FP64 products on the tensor cores (mma.sync
+// m8n8k4; tcgen05 has no FP64 kind) with operands in shared memory.  The
+// next panel's columns get it first (all warps), then warps 4-15 apply it to
+// the remaining columns while warps 0-1 sweep the next panel.
 constexpr int kInvThreads = 512;
-constexpr int kInvGroups = kInvThreads / 128;         // row groups
-constexpr int kInvRows = 128 / kInvGroups;            // rows per thread (32)
+constexpr int kInvN = 128;                            // padded order
+constexpr int kPanel = 16;                            // columns per panel
+constexpr int kLdA = kInvN + 1;                       // odd: a warp reading a column of 32 rows hits distinct banks
+constexpr int kLdX = kPanel + 4;                      // 16-byte rows; 40-word stride puts an 8 x 4 fragment on distinct banks
+constexpr size_t kInvSmem = sizeof(double) * ((size_t)kInvN * kLdA + 3 * (size_t)kInvN * kLdX);
 
-#define AMICA_CASES32(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) \
-    X(13) X(14) X(15) X(16) X(17) X(18) X(19) X(20) X(21) X(22) X(23) X(24) X(25) X(26) X(27)   \
-    X(28) X(29) X(30) X(31)
+__device__ __forceinline__ void bar_panel() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
 
-__device__ __forceinline__ double reg_get(const double (&a)[kInvRows], int i) {
-    double v = 0.0;
-#define AMICA_GET(k) case k: v = a[k]; break;
-    switch (i) { AMICA_CASES32(AMICA_GET) default: break; }
-#undef AMICA_GET
-    return v;
+// D(8x8) += A(8x4) B(4x8) in FP64: lane (g, q) = (lane / 4, lane % 4) holds
+// A(g, q), B(q, g) and D(g, 2q), D(g, 2q + 1)
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
 }
-__device__ __forceinline__ void reg_set(double (&a)[kInvRows], int i, double v) {
-#define AMICA_SET(k) case k: a[k] = v; break;
-    switch (i) { AMICA_CASES32(AMICA_SET) default: break; }
-#undef AMICA_SET
+
+// pivot key of row r holding v (0: not a candidate)
+__device__ __forceinline__ uint32_t pivot_key(double v, bool usable, int r) {
+    return usable ? ((((uint32_t)__double2hiint(v)) & 0x7fffff80u) | (uint32_t)(127 - r)) + 128u : 0u;
+}
+
+// a(i, 8 ct + [0, 8)) for the 16 rows tiles rt0 + [0, 8) <- [i not in P] a + X Pt^T, P the
+// pivot rows of the panel at k0, X its swept columns, Pt the pivot rows' old
+// entries (Pt[j][t] = a_old(p_t, j)); one warp
+__device__ __forceinline__ void block_sweep_strip(double* __restrict__ As, const double* __restrict__ X,
+                                                  const double* __restrict__ Pt, const int* pinv, int k0,
+                                                  int ct, int rt0, int nrt, int lane) {
+    const int g = lane >> 2, q = lane & 3;
+    const int j = 8 * ct + 2 * q;
+    double acc[8][2];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+        if (u < nrt) {
+            const int i = 8 * (rt0 + u) + g;
+            // rows pivoted in this panel have pinv in [k0, k0 + 16); other rows'
+            // pinv is either not set yet or outside that range
+            const bool prow = (unsigned)(pinv[i] - k0) < (unsigned)kPanel;
+            acc[u][0] = prow ? 0.0 : As[i * kLdA + j];
+            acc[u][1] = prow ? 0.0 : As[i * kLdA + j + 1];
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < kPanel; s += 4) {
+        const double bf = Pt[(8 * ct + g) * kLdX + s + q];
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+            if (u < nrt) dmma884(acc[u][0], acc[u][1], X[(8 * (rt0 + u) + g) * kLdX + s + q], bf);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+        if (u < nrt) {
+            const int i = 8 * (rt0 + u) + g;
+            As[i * kLdA + j] = acc[u][0];
+            As[i * kLdA + j + 1] = acc[u][1];
+        }
+    }
 }
 
 __global__ void __launch_bounds__(kInvThreads, 1) k_inverse_derive(
@@ -73,128 +128,225 @@ __global__ void __launch_bounds__(kInvThreads, 1) k_inverse_derive(
     const double* __restrict__ gm, double ldetS, double* __restrict__ W, double* __restrict__ ldet,
     double* __restrict__ ltc64, float* __restrict__ Wf, float* __restrict__ wcf,
     MixParam* __restrict__ mp, int n, int m, int NP, int* err) {
-    extern __shared__ double Ws[];                    // [n][n] row-major W_h, after elimination
-    // colk[buf][g * 32 + i] = a(g + 4 i, k): each thread's rows are contiguous
-    __shared__ __align__(16) double colk[2][128];
-    __shared__ double prow[2][128], pivs[128], wcs[128];
-    __shared__ unsigned long long cval[2][kInvGroups];   // bit pattern of |candidate| (0: none)
-    __shared__ int cidx[2][kInvGroups], perm[128], pinv[128];
-    const int h = blockIdx.x, tid = threadIdx.x;
-    const int g = tid >> 7, col = tid & 127;
+    extern __shared__ __align__(16) double smem_inv[];
+    double* As = smem_inv;                            // a(r, j) at As[r * kLdA + j]
+    double* Xs = As + kInvN * kLdA;                   // swept panels, two buffers: Xs[b & 1][r * kLdX + t]
+    double* Pt = Xs + 2 * kInvN * kLdX;               // Pt[j * kLdX + t] = a(p_t, j) before the panel's update
+    __shared__ __align__(16) double crow_v[2][2][kPanel];   // each panel warp's candidate row
+    __shared__ uint32_t ckey[2][2];
+    __shared__ double cpiv[2][2], cinv[2][2];
+    __shared__ double pivs[kInvN], wcs[kInvN], cperm[kInvN], cs[kInvN];
+    __shared__ float sb_cl2[kMaxMix * kInvN];      // log2 normaliser per (mixture, channel)
+    __shared__ int perm[kInvN], pinv[kInvN];
+    __shared__ int s_bad;
+    __shared__ double s_lgm;
+    const int h = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const double* Ah = A + (size_t)h * n * n;
-    double a[kInvRows];
-#pragma unroll
-    for (int i = 0; i < kInvRows; i++) {
-        const int r = g + kInvGroups * i;
-        a[i] = (r < n && col < n) ? Ah[(size_t)col * n + r] : 0.0;
+    for (int e = tid; e < kInvN * kInvN; e += kInvThreads) {
+        const int j = e >> 7, r = e & (kInvN - 1);
+        As[r * kLdA + j] = (r < n && j < n) ? Ah[(size_t)j * n + r] : 0.0;
     }
-    unsigned used = 0;                                // bit i: row g + 4 i is a pivot row
-    bool bad = false;
-    // Publishing pivot column oc: in each group, the warp that holds column oc
-    // stores it (its owner lane), then picks the group's candidate with a warp
-    // argmax over 32-bit keys: |a| rounded down to 18 mantissa bits above the
-    // row slot, lowest row on ties (the groups' candidates are then compared
-    // exactly).  The candidate's reciprocal is formed here, off the pivot path.
-    __shared__ double cinv[2][kInvGroups];
-    const int warp = tid >> 5, lane = tid & 31;
-    auto publish = [&](int oc, int buf) {
-        if ((warp & 3) != (oc >> 5)) return;          // warp-uniform
-        if (col == oc) {
+    if (tid < kInvN) pinv[tid] = 0x7fffffff;
+    if (tid == 0) s_bad = 0;
+    // panel threads (tid < 64): rows r0 = tid and r1 = tid + 64, not yet pivot rows
+    const int r0 = tid, r1 = tid + 64;
+    bool us0 = r0 < n, us1 = r1 < n;
+    const int npan = (n + kPanel - 1) / kPanel;
+    __syncthreads();
+    for (int b = 0; b <= npan; b++) {
+        const int k0 = kPanel * b;
+        if (b < npan && warp < 2) {
+            double* Xb = Xs + (b & 1) * kInvN * kLdX;
+            double pa[kPanel], pb[kPanel];            // rows r0 and r1
 #pragma unroll
-            for (int i = 0; i < kInvRows; i += 2)
-                *reinterpret_cast<double2*>(&colk[buf][g * kInvRows + i]) = make_double2(a[i], a[i + 1]);
-        }
-        __syncwarp();
-        const double v = colk[buf][g * kInvRows + lane];
-        const bool usable = (g + kInvGroups * lane < n) && !((used >> lane) & 1u);
-        uint32_t key = usable ? ((__float_as_uint((float)fabs(v)) & ~31u) | (uint32_t)(31 - lane)) + 32u : 0u;
+            for (int t = 0; t < kPanel; t++) {
+                pa[t] = As[r0 * kLdA + k0 + t];
+                pb[t] = As[r1 * kLdA + k0 + t];
+            }
+            bool bad = false;
+            uint32_t ka = pivot_key(pa[0], us0, r0), kb = pivot_key(pb[0], us1, r1);
+            uint32_t key = max(ka, kb);
+            double v = kb > ka ? pb[0] : pa[0];
+            double rv = 1.0 / v;
+            uint32_t wkey = __reduce_max_sync(0xffffffffu, key);
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) key = max(key, __shfl_xor_sync(0xffffffffu, key, o));
-        if (lane == 0) {
-            const int ib = 31 - (int)(key & 31u);
-            const double pv = colk[buf][g * kInvRows + ib];
-            cval[buf][g] = key ? (unsigned long long)__double_as_longlong(fabs(pv)) : 0ull;
-            cidx[buf][g] = key ? g + kInvGroups * ib : 0x7fffffff;
-            cinv[buf][g] = key ? 1.0 / pv : 0.0;
-        }
-    };
-    publish(0, 0);
-    for (int k = 0; k < n; k++) {
-        const int buf = k & 1;
-        __syncthreads();
-        // non-negative doubles order like their bit patterns
-        unsigned long long best = cval[buf][0];
-        int p = cidx[buf][0];
-        int gb = 0;
+            for (int t = 0; t < kPanel; t++) {
+                if (k0 + t >= n) break;               // uniform
+                const int buf = t & 1;
+                if (wkey == 0u) {
+                    if (lane == 0) ckey[buf][warp] = 0u;
+                } else if (key == wkey) {             // one thread: the key names its row
+                    const bool second = kb == key;
 #pragma unroll
-        for (int q = 1; q < kInvGroups; q++) {
-            const unsigned long long v = cval[buf][q];
-            const int r = cidx[buf][q];
-            if (v > best || (v == best && r < p)) { best = v; p = r; gb = q; }
-        }
-        if (best == 0ull) { bad = true; break; }     // same decision in every thread
-        const int gp = p % kInvGroups, ip = p / kInvGroups;
-        const double inv = cinv[buf][gb];
-        if (g == gp) {
-            prow[buf][col] = reg_get(a, ip);
-            used |= 1u << ip;
-        }
-        if (tid == 0) { perm[k] = p; pinv[p] = k; pivs[k] = colk[buf][gp * kInvRows + ip]; }
-        __syncthreads();
-        const double pc = prow[buf][col] * inv;       // a(p, col) / piv
-        if (col == k) {
+                    for (int j = 0; j < kPanel; j += 2)
+                        *reinterpret_cast<double2*>(&crow_v[buf][warp][j]) =
+                            second ? make_double2(pb[j], pb[j + 1]) : make_double2(pa[j], pa[j + 1]);
+                    ckey[buf][warp] = key;
+                    cpiv[buf][warp] = v;
+                    cinv[buf][warp] = rv;
+                }
+                bar_panel();
+                const uint32_t kw0 = ckey[buf][0], kw1 = ckey[buf][1];
+                const int wb = kw1 > kw0 ? 1 : 0;     // distinct unless both 0
+                const uint32_t best = max(kw0, kw1);
+                const double piv = wb ? cpiv[buf][1] : cpiv[buf][0];
+                const double inv = wb ? cinv[buf][1] : cinv[buf][0];
+                const int tn = t + 1 < kPanel ? t + 1 : t;
+                const double pn = wb ? crow_v[buf][1][tn] : crow_v[buf][0][tn];
+                if (best == 0u || piv == 0.0) { bad = true; break; }   // same in every panel thread
+                const int p = 127 - (int)((best - 128u) & 127u);
+                const double* pp = crow_v[buf][wb];
+                if (tid == 0) { perm[k0 + t] = p; pinv[p] = k0 + t; pivs[k0 + t] = piv; }
+                const bool pa_is_p = r0 == p, pb_is_p = r1 == p;
+                us0 = us0 && !pa_is_p;
+                us1 = us1 && !pb_is_p;
+                const double fa = pa[t] * inv, fb = pb[t] * inv;
+                if (t + 1 < kPanel) {                 // the next column first, and the next search
+                    pa[t + 1] = fma(-fa, pn, pa[t + 1]);
+                    pb[t + 1] = fma(-fb, pn, pb[t + 1]);
+                    ka = pivot_key(pa[t + 1], us0, r0);
+                    kb = pivot_key(pb[t + 1], us1, r1);
+                    key = max(ka, kb);
+                    v = kb > ka ? pb[t + 1] : pa[t + 1];
+                    rv = 1.0 / v;
+                    wkey = __reduce_max_sync(0xffffffffu, key);
+                }
+                double ppv[kPanel];                   // the pivot row, read once for both rows
 #pragma unroll
-            for (int i = 0; i < kInvRows; i++) a[i] = -a[i] * inv;
-        } else {
-            const double* f = &colk[buf][g * kInvRows];
+                for (int j = 0; j < kPanel; j += 2) {
+                    const double2 d = *reinterpret_cast<const double2*>(pp + j);
+                    ppv[j] = d.x;
+                    ppv[j + 1] = d.y;
+                }
 #pragma unroll
-            for (int i = 0; i < kInvRows; i += 2) {
-                const double2 f2 = *reinterpret_cast<const double2*>(f + i);
-                a[i] = fma(-f2.x, pc, a[i]);
-                a[i + 1] = fma(-f2.y, pc, a[i + 1]);
+                for (int j = 0; j < kPanel; j++)
+                    if (j != t && j != t + 1) {
+                        pa[j] = fma(-fa, ppv[j], pa[j]);
+                        pb[j] = fma(-fb, ppv[j], pb[j]);
+                    }
+                pa[t] = -fa;
+                pb[t] = -fb;
+                if (pa_is_p) {                        // the pivot row: its own entries over the pivot
+#pragma unroll
+                    for (int j = 0; j < kPanel; j++) pa[j] = j == t ? inv : ppv[j] * inv;
+                }
+                if (pb_is_p) {
+#pragma unroll
+                    for (int j = 0; j < kPanel; j++) pb[j] = j == t ? inv : ppv[j] * inv;
+                }
+            }
+            if (bad && tid == 0) s_bad = 1;
+#pragma unroll
+            for (int t = 0; t < kPanel; t++) {
+                As[r0 * kLdA + k0 + t] = pa[t];
+                As[r1 * kLdA + k0 + t] = pb[t];
+            }
+#pragma unroll
+            for (int t = 0; t < kPanel; t += 2) {
+                *reinterpret_cast<double2*>(&Xb[r0 * kLdX + t]) = make_double2(pa[t], pa[t + 1]);
+                *reinterpret_cast<double2*>(&Xb[r1 * kLdX + t]) = make_double2(pb[t], pb[t + 1]);
+            }
+        } else if (b == 0) {
+            // parameter-only work of the E-step constants, off the elimination's path
+            for (int e = tid - 64; e < m * NP; e += kInvThreads - 64) {
+                const int j = e / NP, i = e - j * NP;
+                float cl = 0.f;
+                if (i < n) {
+                    const size_t idx = ((size_t)h * m + j) * n + i;
+                    cl = (float)((log(alpha[idx]) + 0.5 * log(beta[idx]) - M_LN2 -
+                                  lgamma(1.0 + 1.0 / rho[idx])) * 1.4426950408889634);
+                }
+                sb_cl2[e] = cl;
+            }
+            if (tid >= 64 && tid < 64 + kInvN) cs[tid - 64] = tid - 64 < n ? c[(size_t)h * n + tid - 64] : 0.0;
+            if (tid == 64 + kInvN) s_lgm = log(gm[h]);
+        } else if (b >= 1 && (b == npan || warp >= 4)) {
+            // the previous panel's block sweep on the columns outside it and
+            // outside this panel (which got it already), in column strips of 8
+            const int kp = k0 - kPanel;
+            const double* Xp = Xs + ((b - 1) & 1) * kInvN * kLdX;
+            const int w0 = b == npan ? 0 : 4, nw = b == npan ? 16 : 12;
+            for (int ct = warp - w0; ct < kInvN / 8; ct += nw) {
+                const int j0 = 8 * ct;
+                if ((unsigned)(j0 - kp) < (unsigned)kPanel || (unsigned)(j0 - k0) < (unsigned)kPanel) continue;
+                block_sweep_strip(As, Xp, Pt, pinv, kp, ct, 0, 8, lane);
+                block_sweep_strip(As, Xp, Pt, pinv, kp, ct, 8, 8, lane);
             }
         }
-        if (g == gp) reg_set(a, ip, col == k ? inv : pc);
-        if (k + 1 < n) publish(k + 1, buf ^ 1);
+        __syncthreads();
+        if (s_bad || b == npan) break;
+        // Pt for this panel: its pivot rows' entries outside it, now final up to it
+        const int w = min(kPanel, n - k0);
+        for (int e = tid; e < kPanel * kInvN; e += kInvThreads) {
+            const int j = e >> 4, t = e & (kPanel - 1);
+            if ((unsigned)(j - k0) < (unsigned)kPanel) continue;
+            Pt[j * kLdX + t] = t < w ? As[perm[k0 + t] * kLdA + j] : 0.0;
+        }
+        __syncthreads();
+        if (b + 1 < npan) {
+            // the next panel's 16 columns: 2 strips x 16 row tiles, 2 tiles per warp
+            const double* Xb = Xs + (b & 1) * kInvN * kLdX;
+            block_sweep_strip(As, Xb, Pt, pinv, k0, 2 * (b + 1) + (warp & 1), 2 * (warp >> 1), 2, lane);
+        }
+        __syncthreads();
     }
-    if (bad) {
+    if (s_bad) {
         if (tid == 0) atomicOr(err, kErrSingular);
         return;
     }
-    __syncthreads();
-    // W(j, p_k) = a(p_j, k): row-major copy in shared memory and column-major W_h
+    // W(j, q) = a(perm[j], pinv[q]).  W_h column-major: thread j = tid % 128 holds
+    // its row index perm[j] and walks the columns
     double* Wh = W + (size_t)h * n * n;
-#pragma unroll
-    for (int i = 0; i < kInvRows; i++) {
-        const int r = g + kInvGroups * i;
-        if (r < n && col < n) {
-            const int j = pinv[r], kk = perm[col];
-            Ws[j * n + kk] = a[i];
-            Wh[(size_t)kk * n + j] = a[i];
+    {
+        const int j = tid & (kInvN - 1);
+        if (j < n) {
+            const double* Wr = As + perm[j] * kLdA;
+#pragma unroll 4
+            for (int q = tid >> 7; q < n; q += kInvThreads / kInvN) Wh[(size_t)q * n + j] = Wr[pinv[q]];
         }
     }
-    if (tid < n) pivs[tid] = log(fabs(pivs[tid]));
+    if (tid < n) {
+        pivs[tid] = log(fabs(pivs[tid]));
+        cperm[tid] = cs[perm[tid]];                  // c at the column that holds its W column
+    }
     __syncthreads();
-    if (tid == 0) {
+    if (warp == 0) {
         double ld = 0.0;
-        for (int k = 0; k < n; k++) ld += pivs[k];
-        ldet[h] = -ld;
-        ltc64[h] = log(gm[h]) - ld + ldetS;           // src/amica.cu:1009
+        for (int k = lane; k < n; k += 32) ld += pivs[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ld += __shfl_xor_sync(0xffffffffu, ld, o);
+        if (lane == 0) {
+            ldet[h] = -ld;
+            ltc64[h] = s_lgm - ld + ldetS;            // src/amica.cu:1009
+        }
     }
     // E-step constants: W in FP32 (row-major, NP x NP, zero padded), w_c = W c,
     // and per (mixture, channel) sqrt(beta), sqrt(beta)(mu + w_c), the log2
-    // normaliser and rho
-    if (tid < NP) {
-        double wc = 0.0;
-        if (tid < n)
-            for (int k = 0; k < n; k++) wc += Ws[tid * n + k] * c[(size_t)h * n + k];
-        wcs[tid] = wc;
-        wcf[(size_t)h * NP + tid] = (float)wc;
+    // normaliser and rho.  w_c(i) = sum_col a(perm[i], col) c(perm[col]): four
+    // threads per row, each a quarter of the columns
+    {
+        const int i = tid >> 2, part = tid & 3;
+        double s = 0.0;
+        if (i < n) {
+            const double* Wr = As + perm[i] * kLdA;
+#pragma unroll 8
+            for (int col = part; col < n; col += 4) s = fma(Wr[col], cperm[col], s);
+        }
+        s += __shfl_xor_sync(0xffffffffu, s, 1);
+        s += __shfl_xor_sync(0xffffffffu, s, 2);
+        if (part == 0 && i < NP) {
+            wcs[i] = s;
+            wcf[(size_t)h * NP + i] = (float)s;
+        }
     }
     float* Wfh = Wf + (size_t)h * NP * NP;
-    for (int e = tid; e < NP * NP; e += kInvThreads) {
-        const int i = e / NP, k = e - i * NP;
-        Wfh[e] = (i < n && k < n) ? (float)Ws[i * n + k] : 0.f;
+    {
+        // NP divides the block: thread k = tid % NP keeps pinv[k] and walks the rows
+        const int k = tid % NP;
+        const int pk = k < n ? pinv[k] : 0;
+#pragma unroll 4
+        for (int i = tid / NP; i < NP; i += kInvThreads / NP)
+            Wfh[(size_t)i * NP + k] = (i < n && k < n) ? (float)As[perm[i] * kLdA + pk] : 0.f;
     }
     __syncthreads();
     for (int e = tid; e < m * NP; e += kInvThreads) {
@@ -206,8 +358,7 @@ __global__ void __launch_bounds__(kInvThreads, 1) k_inverse_derive(
             const double r = rho[idx];
             q.s = (float)s;
             q.off = (float)(s * (mu[idx] + wcs[i]));
-            q.cl2 = (float)((log(alpha[idx]) + 0.5 * log(beta[idx]) - M_LN2 - lgamma(1.0 + 1.0 / r)) *
-                            1.4426950408889634);
+            q.cl2 = sb_cl2[e];
             q.rho = (float)r;
         } else {
             q.s = 0.f; q.off = 0.f; q.cl2 = 0.f; q.rho = 1.f;
@@ -818,11 +969,11 @@ cudaError_t launch_prep(const MStepBuffers& b, const MStepCfgHost& h, cudaStream
                                       b.ldet, b.ltc64, b.Wf, b.wcf, b.mp, h.n, h.m, h.NP);
         return cudaGetLastError();
     }
-    const size_t smem = sizeof(double) * (size_t)h.n * h.n;
+    if (h.NP > 128 || kInvThreads % h.NP || h.m > kMaxMix) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(k_inverse_derive, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+                                         (int)kInvSmem);
     if (e != cudaSuccess) return e;
-    k_inverse_derive<<<h.M, kInvThreads, smem, st>>>(b.A, b.c, b.alpha, b.mu, b.beta, b.rho, b.gm,
+    k_inverse_derive<<<h.M, kInvThreads, kInvSmem, st>>>(b.A, b.c, b.alpha, b.mu, b.beta, b.rho, b.gm,
                                                      h.ldetS, b.W, b.ldet, b.ltc64, b.Wf, b.wcf, b.mp,
                                                      h.n, h.m, h.NP, b.err);
     return cudaGetLastError();
