@@ -369,11 +369,11 @@ __global__ void __launch_bounds__(kInvThreads, 1) k_inverse_derive(
 
 // ---------------------------------------------------------------------------
 // k_inverse_gj: W_h = A_h^{-1} and log|pivots| for 128 < n <= 256, where the
-// n x n FP64 matrix no longer fits in one SM.  The same Gauss-Jordan
-// elimination as k_inverse_derive (partial pivoting, no row interchanges,
-// largest |a(r, k)| over the unused rows, lowest row on ties, exact compares)
-// on a column-major working copy in global memory (L2-resident); one CTA of
-// 1024 threads per model, the pivot column and row staged in shared memory.
+// n x n FP64 matrix no longer fits in one SM.  Gauss-Jordan elimination with
+// partial pivoting and no row interchanges (largest |a(r, k)| over the unused
+// rows, lowest row on ties, exact compares) on a column-major working copy in
+// global memory (L2-resident); one CTA of 1024 threads per model, the pivot
+// column and row staged in shared memory.
 constexpr int kGJThreads = 1024;
 constexpr int kMaxN = 256;
 __global__ void __launch_bounds__(kGJThreads, 1) k_inverse_gj(const double* __restrict__ A,
