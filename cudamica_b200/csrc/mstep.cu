@@ -368,74 +368,215 @@ __global__ void __launch_bounds__(kInvThreads, 1) k_inverse_derive(
 }
 
 // ---------------------------------------------------------------------------
-// k_inverse_gj: W_h = A_h^{-1} and log|pivots| for 128 < n <= 256, where the
-// n x n FP64 matrix no longer fits in one SM.  Gauss-Jordan elimination with
-// partial pivoting and no row interchanges (largest |a(r, k)| over the unused
-// rows, lowest row on ties, exact compares) on a column-major working copy in
-// global memory (L2-resident); one CTA of 1024 threads per model, the pivot
-// column and row staged in shared memory.
-constexpr int kGJThreads = 1024;
+// k_inverse_big: W_h = A_h^{-1} and log|pivots| for 128 < n <= 256, where the
+// n x n FP64 matrix no longer fits in one SM's shared memory.  The blocked
+// Gauss-Jordan elimination of k_inverse_derive (16-column panels, the same
+// pivot keys with 8 row bits, the block sweep on the FP64 tensor cores with
+// look-ahead) on a row-major working copy in global memory (L2-resident, 512
+// KB at n = 256); one CTA of 512 threads per model.  Warps 0-3 sweep a panel
+// (thread r holds rows r and r + 128, one 128-thread barrier per pivot);
+// warps 4-15 apply the previous panel's block sweep to the other columns,
+// reading and writing their accumulators in global memory.
 constexpr int kMaxN = 256;
-__global__ void __launch_bounds__(kGJThreads, 1) k_inverse_gj(const double* __restrict__ A,
-                                                             double* __restrict__ work,
-                                                             double* __restrict__ W,
-                                                             double* __restrict__ pivlog, int n,
-                                                             int* err) {
-    const int h = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    double* a = work + (size_t)h * n * n;
-    const double* Ah = A + (size_t)h * n * n;
-    __shared__ double f[kMaxN], prow[kMaxN], wv[32];
-    __shared__ int perm[kMaxN], pinv[kMaxN], wi[32];
-    __shared__ unsigned char used[kMaxN];
-    __shared__ int s_p, s_bad;
-    __shared__ double s_inv;
-    for (int e = tid; e < n * n; e += kGJThreads) a[e] = Ah[e];
-    for (int i = tid; i < n; i += kGJThreads) used[i] = 0;
-    if (tid == 0) s_bad = 0;
-    __syncthreads();
-    for (int k = 0; k < n; k++) {
-        double v = -1.0;
-        int r = 0x7fffffff;
-        if (tid < n && !used[tid]) { v = fabs(a[(size_t)k * n + tid]); r = tid; }
+constexpr int kBigN = kMaxN;
+constexpr size_t kBigSmem = sizeof(double) * 3 * (size_t)kBigN * kLdX;
+
+__device__ __forceinline__ void bar_panel4() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+__device__ __forceinline__ uint32_t pivot_key8(double v, bool usable, int r) {
+    return usable ? ((((uint32_t)__double2hiint(v)) & 0x7fffff00u) | (uint32_t)(255 - r)) + 256u : 0u;
+}
+
+// the global-memory form of block_sweep_strip: a(i, 8 ct + [0, 8)) for the
+// row tiles rt0 + [0, nrt) of G (row-major, stride n; rows and columns at and
+// beyond n are skipped)
+__device__ __forceinline__ void block_sweep_strip_g(double* __restrict__ G, int n, const double* __restrict__ X,
+                                                    const double* __restrict__ Pt, const int* pinv, int k0,
+                                                    int ct, int rt0, int nrt, int lane) {
+    const int g = lane >> 2, q = lane & 3;
+    const int j = 8 * ct + 2 * q;
+    const bool ok0 = j < n, ok1 = j + 1 < n;
+    double acc[8][2];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
-            const int r2 = __shfl_xor_sync(0xffffffffu, r, o);
-            if (v2 > v || (v2 == v && r2 < r)) { v = v2; r = r2; }
+    for (int u = 0; u < 8; u++) {
+        if (u < nrt) {
+            const int i = 8 * (rt0 + u) + g;
+            const bool ok = i < n && !((unsigned)(pinv[i] - k0) < (unsigned)kPanel);
+            acc[u][0] = ok && ok0 ? G[(size_t)i * n + j] : 0.0;
+            acc[u][1] = ok && ok1 ? G[(size_t)i * n + j + 1] : 0.0;
         }
-        if (lane == 0) { wv[warp] = v; wi[warp] = r; }
-        __syncthreads();
-        if (tid == 0) {
-            double bv = wv[0];
-            int br = wi[0];
-            for (int q = 1; q < kGJThreads / 32; q++)
-                if (wv[q] > bv || (wv[q] == bv && wi[q] < br)) { bv = wv[q]; br = wi[q]; }
-            if (!(bv > 0.0)) {
-                s_bad = 1;
-            } else {
-                const double piv = a[(size_t)k * n + br];
-                s_p = br;
-                s_inv = 1.0 / piv;
-                perm[k] = br;
-                pinv[br] = k;
-                used[br] = 1;
-                pivlog[(size_t)h * n + k] = log(fabs(piv));
+    }
+#pragma unroll
+    for (int s = 0; s < kPanel; s += 4) {
+        const double bf = Pt[(8 * ct + g) * kLdX + s + q];
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+            if (u < nrt) dmma884(acc[u][0], acc[u][1], X[(8 * (rt0 + u) + g) * kLdX + s + q], bf);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+        if (u < nrt) {
+            const int i = 8 * (rt0 + u) + g;
+            if (i < n) {
+                if (ok0) G[(size_t)i * n + j] = acc[u][0];
+                if (ok1) G[(size_t)i * n + j + 1] = acc[u][1];
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kInvThreads, 1) k_inverse_big(const double* __restrict__ A,
+                                                               double* __restrict__ work,
+                                                               double* __restrict__ W,
+                                                               double* __restrict__ pivlog, int n,
+                                                               int* err) {
+    extern __shared__ __align__(16) double smem_big[];
+    double* Xs = smem_big;                            // swept panels, two buffers of 256 x kLdX
+    double* Pt = Xs + 2 * kBigN * kLdX;               // Pt[j * kLdX + t] = a(p_t, j) before the panel's update
+    __shared__ __align__(16) double crow_v[2][4][kPanel];
+    __shared__ uint32_t ckey[2][4];
+    __shared__ double cpiv[2][4], cinv[2][4];
+    __shared__ double pivs[kBigN];
+    __shared__ int perm[kBigN], pinv[kBigN];
+    __shared__ int s_bad;
+    const int h = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const double* Ah = A + (size_t)h * n * n;         // column-major a(r, j) = Ah[j n + r]
+    double* G = work + (size_t)h * n * n;             // row-major a(r, j) = G[r n + j]
+    for (int e = tid; e < n * n; e += kInvThreads) {
+        const int j = e / n, r = e - j * n;
+        G[(size_t)r * n + j] = Ah[e];
+    }
+    if (tid < kBigN) pinv[tid] = 0x7fffffff;
+    if (tid == 0) s_bad = 0;
+    const int r0 = tid, r1 = tid + 128;               // panel threads (tid < 128)
+    bool us0 = r0 < n, us1 = r1 < n;
+    const int npan = (n + kPanel - 1) / kPanel, ncs = (n + 7) / 8;
+    __syncthreads();
+    for (int b = 0; b <= npan; b++) {
+        const int k0 = kPanel * b;
+        if (b < npan && warp < 4) {
+            double* Xb = Xs + (b & 1) * kBigN * kLdX;
+            double pa[kPanel], pb[kPanel];
+#pragma unroll
+            for (int t = 0; t < kPanel; t++) {
+                const bool cok = k0 + t < n;
+                pa[t] = cok && r0 < n ? G[(size_t)r0 * n + k0 + t] : 0.0;
+                pb[t] = cok && r1 < n ? G[(size_t)r1 * n + k0 + t] : 0.0;
+            }
+            bool bad = false;
+            uint32_t ka = pivot_key8(pa[0], us0, r0), kb = pivot_key8(pb[0], us1, r1);
+            uint32_t key = max(ka, kb);
+            double v = kb > ka ? pb[0] : pa[0];
+            double rv = 1.0 / v;
+            uint32_t wkey = __reduce_max_sync(0xffffffffu, key);
+#pragma unroll
+            for (int t = 0; t < kPanel; t++) {
+                if (k0 + t >= n) break;               // uniform
+                const int buf = t & 1;
+                if (wkey == 0u) {
+                    if (lane == 0) ckey[buf][warp] = 0u;
+                } else if (key == wkey) {             // one thread: the key names its row
+                    const bool second = kb == key;
+#pragma unroll
+                    for (int j = 0; j < kPanel; j += 2)
+                        *reinterpret_cast<double2*>(&crow_v[buf][warp][j]) =
+                            second ? make_double2(pb[j], pb[j + 1]) : make_double2(pa[j], pa[j + 1]);
+                    ckey[buf][warp] = key;
+                    cpiv[buf][warp] = v;
+                    cinv[buf][warp] = rv;
+                }
+                bar_panel4();
+                const int tn = t + 1 < kPanel ? t + 1 : t;
+                uint32_t best = ckey[buf][0];
+                int wb = 0;
+                double piv = cpiv[buf][0], inv = cinv[buf][0], pn = crow_v[buf][0][tn];
+#pragma unroll
+                for (int qq = 1; qq < 4; qq++) {
+                    const uint32_t kq = ckey[buf][qq];
+                    const double pq = cpiv[buf][qq], iq = cinv[buf][qq], nq = crow_v[buf][qq][tn];
+                    if (kq > best) { best = kq; wb = qq; piv = pq; inv = iq; pn = nq; }
+                }
+                if (best == 0u || piv == 0.0) { bad = true; break; }   // same in every panel thread
+                const int p = 255 - (int)((best - 256u) & 255u);
+                const double* pp = crow_v[buf][wb];
+                if (tid == 0) { perm[k0 + t] = p; pinv[p] = k0 + t; pivs[k0 + t] = piv; }
+                const bool pa_is_p = r0 == p, pb_is_p = r1 == p;
+                us0 = us0 && !pa_is_p;
+                us1 = us1 && !pb_is_p;
+                const double fa = pa[t] * inv, fb = pb[t] * inv;
+                if (t + 1 < kPanel) {                 // the next column first, and the next search
+                    pa[t + 1] = fma(-fa, pn, pa[t + 1]);
+                    pb[t + 1] = fma(-fb, pn, pb[t + 1]);
+                    ka = pivot_key8(pa[t + 1], us0, r0);
+                    kb = pivot_key8(pb[t + 1], us1, r1);
+                    key = max(ka, kb);
+                    v = kb > ka ? pb[t + 1] : pa[t + 1];
+                    rv = 1.0 / v;
+                    wkey = __reduce_max_sync(0xffffffffu, key);
+                }
+                double ppv[kPanel];                   // the pivot row, read once for both rows
+#pragma unroll
+                for (int j = 0; j < kPanel; j += 2) {
+                    const double2 d = *reinterpret_cast<const double2*>(pp + j);
+                    ppv[j] = d.x;
+                    ppv[j + 1] = d.y;
+                }
+#pragma unroll
+                for (int j = 0; j < kPanel; j++)
+                    if (j != t && j != t + 1) {
+                        pa[j] = fma(-fa, ppv[j], pa[j]);
+                        pb[j] = fma(-fb, ppv[j], pb[j]);
+                    }
+                pa[t] = -fa;
+                pb[t] = -fb;
+                if (pa_is_p) {                        // the pivot row: its own entries over the pivot
+#pragma unroll
+                    for (int j = 0; j < kPanel; j++) pa[j] = j == t ? inv : ppv[j] * inv;
+                }
+                if (pb_is_p) {
+#pragma unroll
+                    for (int j = 0; j < kPanel; j++) pb[j] = j == t ? inv : ppv[j] * inv;
+                }
+            }
+            if (bad && tid == 0) s_bad = 1;
+#pragma unroll
+            for (int t = 0; t < kPanel; t++) {
+                if (k0 + t < n) {
+                    if (r0 < n) G[(size_t)r0 * n + k0 + t] = pa[t];
+                    if (r1 < n) G[(size_t)r1 * n + k0 + t] = pb[t];
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < kPanel; t += 2) {
+                *reinterpret_cast<double2*>(&Xb[r0 * kLdX + t]) = make_double2(pa[t], pa[t + 1]);
+                *reinterpret_cast<double2*>(&Xb[r1 * kLdX + t]) = make_double2(pb[t], pb[t + 1]);
+            }
+        } else if (b >= 1 && (b == npan || warp >= 4)) {
+            // the previous panel's block sweep outside it and outside this panel
+            const int kp = k0 - kPanel;
+            const double* Xp = Xs + ((b - 1) & 1) * kBigN * kLdX;
+            const int w0 = b == npan ? 0 : 4, nw = b == npan ? 16 : 12;
+            for (int ct = warp - w0; ct < ncs; ct += nw) {
+                const int j0 = 8 * ct;
+                if ((unsigned)(j0 - kp) < (unsigned)kPanel || (unsigned)(j0 - k0) < (unsigned)kPanel) continue;
+                for (int rt0 = 0; 8 * rt0 < n; rt0 += 8) block_sweep_strip_g(G, n, Xp, Pt, pinv, kp, ct, rt0, 8, lane);
             }
         }
         __syncthreads();
-        if (s_bad) break;
-        const int p = s_p;
-        const double inv = s_inv;
-        if (tid < n) {
-            f[tid] = a[(size_t)k * n + tid];
-            prow[tid] = a[(size_t)tid * n + p];
+        if (s_bad || b == npan) break;
+        // Pt for this panel: its pivot rows' entries outside it, now final up to it
+        const int w = min(kPanel, n - k0);
+        for (int e = tid; e < kPanel * kBigN; e += kInvThreads) {
+            const int j = e >> 4, t = e & (kPanel - 1);
+            if ((unsigned)(j - k0) < (unsigned)kPanel) continue;
+            Pt[j * kLdX + t] = t < w && j < n ? G[(size_t)perm[k0 + t] * n + j] : 0.0;
         }
         __syncthreads();
-        for (int e = tid; e < n * n; e += kGJThreads) {
-            const int j = e / n, rr = e - j * n;
-            if (j == k) a[e] = (rr == p) ? inv : -f[rr] * inv;
-            else if (rr == p) a[e] = prow[j] * inv;
-            else a[e] = fma(-f[rr], prow[j] * inv, a[e]);
+        if (b + 1 < npan) {
+            // the next panel's columns: 2 strips x 32 row tiles, 4 tiles per warp
+            const double* Xb = Xs + (b & 1) * kBigN * kLdX;
+            const int rt0 = 4 * (warp >> 1);
+            if (8 * rt0 < n) block_sweep_strip_g(G, n, Xb, Pt, pinv, k0, 2 * (b + 1) + (warp & 1), rt0, 4, lane);
         }
         __syncthreads();
     }
@@ -443,12 +584,16 @@ __global__ void __launch_bounds__(kGJThreads, 1) k_inverse_gj(const double* __re
         if (tid == 0) atomicOr(err, kErrSingular);
         return;
     }
-    // W(j, p_k) = a(p_j, k), W column-major
+    // W(j, q) = a(perm[j], pinv[q]), column-major W_h
     double* Wh = W + (size_t)h * n * n;
-    for (int e = tid; e < n * n; e += kGJThreads) {
-        const int k = e / n, rr = e - k * n;
-        Wh[(size_t)perm[k] * n + pinv[rr]] = a[e];
+    {
+        const int j = tid & (kBigN - 1);
+        if (j < n) {
+            const double* Gr = G + (size_t)perm[j] * n;
+            for (int q = tid >> 8; q < n; q += kInvThreads / kBigN) Wh[(size_t)q * n + j] = Gr[pinv[q]];
+        }
     }
+    for (int k = tid; k < n; k += kInvThreads) pivlog[(size_t)h * n + k] = log(fabs(pivs[k]));
 }
 
 // k_derive: log|det W_h|, the Lt constant and the FP32 E-step constants from a
@@ -964,7 +1109,10 @@ cudaError_t launch_prep(const MStepBuffers& b, const MStepCfgHost& h, cudaStream
     if (h.n > 128) {
         if (!b.gj) return cudaErrorInvalidValue;
         double* pivlog = b.gj + (size_t)h.M * h.n * h.n;
-        k_inverse_gj<<<h.M, kGJThreads, 0, st>>>(b.A, b.gj, b.W, pivlog, h.n, b.err);
+        cudaError_t e = cudaFuncSetAttribute(k_inverse_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kBigSmem);
+        if (e != cudaSuccess) return e;
+        k_inverse_big<<<h.M, kInvThreads, kBigSmem, st>>>(b.A, b.gj, b.W, pivlog, h.n, b.err);
         k_derive<<<h.M, 256, 0, st>>>(b.W, pivlog, b.c, b.alpha, b.mu, b.beta, b.rho, b.gm, h.ldetS,
                                       b.ldet, b.ltc64, b.Wf, b.wcf, b.mp, h.n, h.m, h.NP);
         return cudaGetLastError();
