@@ -361,7 +361,7 @@ def profile_case(args):
     else:
         x, A0, c0 = make_data()
         n, M, m = WORKLOAD["n"], WORKLOAD["M"], WORKLOAD["m"]
-    for precision in ((0,) if n > 128 else (1, 0)):
+    for precision in (1, 0):
         eng = Amica(n, T, M, m, precision=precision, device=0)
         eng.load_data(np.ascontiguousarray(x[:T]))
         eng.preprocess()

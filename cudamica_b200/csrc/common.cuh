@@ -91,6 +91,11 @@ struct EStepArgs {
     int ntiles, nclusters;
     int update_rho;
     int grad_mode;           // 1: beta-denominator slot holds sum u*f'*y for every rho (adjoint)
+    // density-only form (contractions done outside the kernel): b = W x and g
+    // per sample, both [T][M][NP] with a row of ldb floats per sample
+    const float* bext;
+    float* gout;
+    int ldb;
 };
 
 // The cohort E-step (one persistent launch over many single-model fits): a

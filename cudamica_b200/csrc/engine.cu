@@ -3,7 +3,9 @@
 //
 // One iteration is a fixed sequence of kernels on the context's stream:
 //   k_inverse_derive (FP64 inverse, log-det, E-step constants)
-//   -> fused E-step (plain FP32 or tcgen05 TF32)
+//   -> fused E-step (plain FP32 or tcgen05 TF32; above 128 channels the
+//      mixed form is the split one: b = W x as TF32 tensor-core GEMMs, the
+//      density-only E-step, then Psi = sum g x^T as TF32 GEMMs)
 //   -> k_reduce + k_finalize (deterministic FP64 reduction of per-CTA sums)
 //   -> k_mstep_params -> k_ctrl -> k_gemm64 (A update) -> k_reparm
 //   (-> k_reject on schedule)
@@ -20,6 +22,8 @@
 #include <string>
 #include <vector>
 
+#include <cublas_v2.h>
+
 #include "amica_b200.h"
 #include "common.cuh"
 
@@ -30,6 +34,11 @@ int plain_partial_groups(int n);
 int plain_max_clusters(int n, int m, int M);
 int plain_tile_samples();
 cudaError_t launch_estep_plain(const EStepArgs& a, int NP, int nclusters, cudaStream_t st);
+bool plain_ext_supported(int n);
+int plain_ext_max_clusters(int m, int M);
+cudaError_t launch_estep_plain_ext(const EStepArgs& a, int nclusters, cudaStream_t st);
+cudaError_t launch_split_w(const float* Wf, float* whi, float* wlo, int64_t len, cudaStream_t st);
+cudaError_t launch_psi_add(const float* psi32, double* partial, int n, int m, int M, cudaStream_t st);
 // estep_tc.cu
 int tc_supported(int n, int m, int M);
 int tc_max_clusters(int n, int m, int M);
@@ -75,6 +84,14 @@ struct amica_ctx {
     int n = 0, M = 0, m = 0, NP = 0, S = 0;
     int64_t T = 0;
     bool use_tc = false;
+    // split mixed form (128 < n <= 256): TF32 GEMMs around the density-only E-step
+    bool use_split = false;
+    cublasHandle_t cublas = nullptr;
+    void* cublas_ws = nullptr;                    // the handle's workspace (graph capture)
+    float *d_B = nullptr, *d_G = nullptr;         // T x M x NP: b = W x and g per sample
+    float *d_Whi = nullptr, *d_Wlo = nullptr;     // M x NP x NP TF32 split of W
+    float* d_psi32 = nullptr;                     // M x n x n: one sample chunk of Psi
+    int adj_nclusters = 0;                        // grid of the plain gradient kernel (split form)
     int nclusters = 0, ntiles = 0, nslots = 0;   // nslots: partial-sum slots per model
     int nclusters_cap = 0;                        // grid the partial-sum buffer was sized for
     bool have_data = false, have_x = false, have_init = false, have_estep = false;
@@ -189,13 +206,56 @@ EStepArgs estep_args(amica_ctx* c) {
     a.ntiles = c->ntiles;
     a.nclusters = c->nclusters;
     a.update_rho = (int)c->cfg.update_rho;
+    if (c->use_split) {
+        a.bext = c->d_B;
+        a.gout = c->d_G;
+        a.ldb = c->M * c->NP;
+    }
     return a;
+}
+
+// Samples per Psi GEMM: each chunk is summed in FP32 on the tensor cores and
+// added into the FP64 partial sums.
+constexpr int64_t kPsiChunk = 262144;
+
+#define CB(x)                                                                       \
+    do {                                                                            \
+        if ((x) != CUBLAS_STATUS_SUCCESS) return AMICA_ERR_CUDA;                    \
+    } while (0)
+
+// The split form's E-step: W -> (W_hi, W_lo), b = W_hi x + W_lo x, the
+// density-only kernel, Psi = sum g x^T per chunk of samples (TF32 GEMMs with
+// FP32 accumulation; W_hi has no bits below TF32, so only W_lo and the data
+// are rounded).
+int enqueue_split_estep(amica_ctx* c, const EStepArgs& a) {
+    const int M = c->M, NP = c->NP, n = c->n;
+    const int T = (int)c->T;
+    const float one = 1.f, zero = 0.f;
+    CK(launch_split_w(c->b.Wf, c->d_Whi, c->d_Wlo, (int64_t)M * NP * NP, c->st));
+    CB(cublasGemmEx(c->cublas, CUBLAS_OP_T, CUBLAS_OP_N, M * NP, T, NP, &one, c->d_Whi, CUDA_R_32F, NP,
+                    c->d_x, CUDA_R_32F, NP, &zero, c->d_B, CUDA_R_32F, M * NP,
+                    CUBLAS_COMPUTE_32F_FAST_TF32, CUBLAS_GEMM_DEFAULT));
+    CB(cublasGemmEx(c->cublas, CUBLAS_OP_T, CUBLAS_OP_N, M * NP, T, NP, &one, c->d_Wlo, CUDA_R_32F, NP,
+                    c->d_x, CUDA_R_32F, NP, &one, c->d_B, CUDA_R_32F, M * NP,
+                    CUBLAS_COMPUTE_32F_FAST_TF32, CUBLAS_GEMM_DEFAULT));
+    CK(launch_estep_plain_ext(a, c->nclusters, c->st));
+    for (int64_t t0 = 0; t0 < c->T; t0 += kPsiChunk) {
+        const int k = (int)std::min<int64_t>(kPsiChunk, c->T - t0);
+        CB(cublasGemmStridedBatchedEx(c->cublas, CUBLAS_OP_N, CUBLAS_OP_T, n, n, k, &one,
+                                      c->d_G + t0 * (int64_t)M * NP, CUDA_R_32F, M * NP, NP,
+                                      c->d_x + t0 * NP, CUDA_R_32F, NP, 0, &zero, c->d_psi32,
+                                      CUDA_R_32F, n, (long long)n * n, M, CUBLAS_COMPUTE_32F_FAST_TF32,
+                                      CUBLAS_GEMM_DEFAULT));
+        CK(launch_psi_add(c->d_psi32, c->b.partial, n, c->m, M, c->st));
+    }
+    return AMICA_OK;
 }
 
 int enqueue_estep(amica_ctx* c) {
     CK(launch_prep(c->b, c->hc, c->st));
     EStepArgs a = estep_args(c);
-    if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st));
+    if (c->use_split) TRY(enqueue_split_estep(c, a));
+    else if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st));
     else CK(launch_estep_plain(a, c->NP, c->nclusters, c->st));
     CK(launch_reduce_finalize(c->b, c->hc, c->nslots, c->st));
     return AMICA_OK;
@@ -205,7 +265,10 @@ int enqueue_estep(amica_ctx* c) {
 // (+ phi from Psi in the plain form), params, ctrl, A update (when A is
 // updated), reparametrisation (+ rejection when enabled).
 int launches_per_iteration(const amica_ctx* c) {
-    return 7 + (c->hc.psi_is_phi ? 0 : 1) + (c->hc.update_A ? 1 : 0) + (c->hc.do_reject ? 1 : 0);
+    // the split form adds the W split and one Psi add per sample chunk (its
+    // GEMMs are library kernels and not counted)
+    const int split = c->use_split ? 1 + (int)((c->T + kPsiChunk - 1) / kPsiChunk) : 0;
+    return 7 + split + (c->hc.psi_is_phi ? 0 : 1) + (c->hc.update_A ? 1 : 0) + (c->hc.do_reject ? 1 : 0);
 }
 
 int enqueue_iteration(amica_ctx* c) {
@@ -337,9 +400,13 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     CK(cudaEventCreate(&c->ev1));
 
     c->use_tc = (cfg->precision == AMICA_PREC_MIXED) && tc_supported((int)n, (int)m, (int)M);
+    c->use_split = (cfg->precision == AMICA_PREC_MIXED) && !c->use_tc && plain_ext_supported((int)n) &&
+                   T <= 0x7fffffff;
     c->S = c->use_tc ? tc_tile_samples((int)n) : plain_tile_samples();
     c->ntiles = (int)((T + c->S - 1) / c->S);
-    int maxcl = c->use_tc ? tc_max_clusters((int)n, (int)m, (int)M) : plain_max_clusters((int)n, (int)m, (int)M);
+    int maxcl = c->use_tc      ? tc_max_clusters((int)n, (int)m, (int)M)
+                : c->use_split ? plain_ext_max_clusters((int)m, (int)M)
+                               : plain_max_clusters((int)n, (int)m, (int)M);
     if (maxcl <= 0) { amica_destroy(c); return AMICA_ERR_UNSUPPORTED; }
     // partial-sum slots are sized for the full grid so that amica_set_grid can
     // move between any grid sizes later
@@ -370,9 +437,17 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     AL(b.beta, M * mn); AL(b.rho, M * mn); AL(b.gm, M); AL(b.W, M * nn); AL(b.ldet, M);
     AL(b.ltc64, M);
     PartLayout PL{(int)n, (int)m};
-    const int groups = c->use_tc ? tc_partial_groups((int)n) : plain_partial_groups((int)n);
+    const int groups = c->use_tc ? tc_partial_groups((int)n) : c->use_split ? 1 : plain_partial_groups((int)n);
     c->nslots = c->nclusters * groups;
-    AL(b.partial, (size_t)c->nclusters_cap * groups * M * PL.stride());
+    size_t pslots = (size_t)c->nclusters_cap * groups;
+    if (c->use_split) {
+        // its adjoint runs the plain gradient kernel (channel-split clusters)
+        const int pcl = plain_max_clusters((int)n, (int)m, (int)M);
+        if (pcl <= 0) { amica_destroy(c); return AMICA_ERR_UNSUPPORTED; }
+        c->adj_nclusters = pcl < c->ntiles ? pcl : c->ntiles;
+        pslots = std::max(pslots, (size_t)c->adj_nclusters * plain_partial_groups((int)n));
+    }
+    AL(b.partial, pslots * M * PL.stride());
     AL(b.raw, M * (size_t)PL.stride());
     AL(b.stats, (size_t)amica_stats_len(n, M, m));
     AL(b.work, M * 4 * n);
@@ -394,6 +469,19 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     AL(c->d_ldetS, 1);
     c->backup_len = param_len(c) + (sizeof(Ctrl) + 7) / 8;
     AL(c->d_backup, c->backup_len);
+    if (c->use_split) {
+        AL(c->d_B, (size_t)T * M * NP); AL(c->d_G, (size_t)T * M * NP);
+        AL(c->d_Whi, (size_t)M * NP * NP); AL(c->d_Wlo, (size_t)M * NP * NP);
+        AL(c->d_psi32, (size_t)M * nn);
+        const size_t ws = (size_t)32 << 20;
+        if (cudaMalloc(&c->cublas_ws, ws) != cudaSuccess) { amica_destroy(c); return AMICA_ERR_CUDA; }
+        if (cublasCreate(&c->cublas) != CUBLAS_STATUS_SUCCESS ||
+            cublasSetStream(c->cublas, c->st) != CUBLAS_STATUS_SUCCESS ||
+            cublasSetWorkspace(c->cublas, c->cublas_ws, ws) != CUBLAS_STATUS_SUCCESS) {
+            amica_destroy(c);
+            return AMICA_ERR_CUDA;
+        }
+    }
 #undef AL
     CK(cudaMemsetAsync(c->d_keep, 1, T, c->st));
     CK(cudaMallocHost(&c->h_ctrl, sizeof(Ctrl)));
@@ -413,7 +501,9 @@ int amica_destroy(amica_ctx* c) {
                     c->b.work, c->b.chunk, c->b.gj, c->b.bflag, c->b.use_newton, c->b.Wf, c->b.wcf,
                     c->b.mp, c->b.ctrl, c->b.hist, c->b.err, c->d_keep, c->d_Lt, c->d_P, c->d_x,
                     c->d_rawx, c->d_means, c->d_sphere, c->d_cov, c->d_evwork, c->d_ldetS,
-                    c->d_backup, c->d_gradp, c->d_grad};
+                    c->d_backup, c->d_gradp, c->d_grad, c->d_B, c->d_G, c->d_Whi, c->d_Wlo,
+                    c->d_psi32, c->cublas_ws};
+    if (c->cublas) cublasDestroy(c->cublas);
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_ctrl) cudaFreeHost(c->h_ctrl);
@@ -427,7 +517,7 @@ int amica_destroy(amica_ctx* c) {
 
 const char* amica_kernel_name(amica_ctx* c) {
     if (!c) return "";
-    return c->use_tc ? "tc_tf32" : "plain_fp32";
+    return c->use_tc ? "tc_tf32" : c->use_split ? "split_tf32" : "plain_fp32";
 }
 
 static int load_raw(amica_ctx* c, const float* x, int64_t n, int64_t T, cudaMemcpyKind kind) {
@@ -454,7 +544,7 @@ int amica_preprocess(amica_ctx* c) {
     if (!c->have_data) return AMICA_ERR_STATE;
     CK(cudaSetDevice(c->dev));
     CK(launch_preprocess(c->d_rawx, c->T, c->n, (int)c->cfg.do_sphere, c->d_means, c->d_cov,
-                         c->d_sphere, c->d_evwork, c->d_ldetS, c->d_x, c->NP, c->use_tc ? 1 : 0,
+                         c->d_sphere, c->d_evwork, c->d_ldetS, c->d_x, c->NP, (c->use_tc || c->use_split) ? 1 : 0,
                          c->b.err, c->st));
     double ld = 0.0;
     CK(cudaMemcpyAsync(&ld, c->d_ldetS, sizeof(double), cudaMemcpyDeviceToHost, c->st));
@@ -474,7 +564,7 @@ int amica_set_sphered(amica_ctx* c, const double* xs, const double* means, const
     const size_t bytes = sizeof(double) * (size_t)c->T * c->n;
     CK(cudaMalloc(&tmp, bytes));
     CK(cudaMemcpyAsync(tmp, xs, bytes, cudaMemcpyHostToDevice, c->st));
-    CK(launch_convert_sphered(tmp, c->T, c->n, c->d_x, c->NP, c->use_tc ? 1 : 0, c->st));
+    CK(launch_convert_sphered(tmp, c->T, c->n, c->d_x, c->NP, (c->use_tc || c->use_split) ? 1 : 0, c->st));
     if (means) CK(cudaMemcpyAsync(c->d_means, means, sizeof(double) * c->n, cudaMemcpyHostToDevice, c->st));
     if (sphere) CK(cudaMemcpyAsync(c->d_sphere, sphere, sizeof(double) * c->n * c->n, cudaMemcpyHostToDevice, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -639,14 +729,16 @@ int amica_set_grid(amica_ctx* c, int64_t max_clusters, int64_t* nclusters) {
     if (!c || max_clusters < 0) return AMICA_ERR_INVALIDPARAM;
     if (c->pending >= 0) return AMICA_ERR_STATE;
     CK(cudaSetDevice(c->dev));
-    int maxcl = c->use_tc ? tc_max_clusters(c->n, c->m, c->M) : plain_max_clusters(c->n, c->m, c->M);
+    int maxcl = c->use_tc      ? tc_max_clusters(c->n, c->m, c->M)
+                : c->use_split ? plain_ext_max_clusters(c->m, c->M)
+                               : plain_max_clusters(c->n, c->m, c->M);
     if (maxcl <= 0) return AMICA_ERR_UNSUPPORTED;
     if (max_clusters > 0 && max_clusters < maxcl) maxcl = (int)max_clusters;
     const int ncl = maxcl < c->ntiles ? maxcl : c->ntiles;
     // the partial-sum slots were sized for the largest grid at creation
     if (ncl > c->nclusters_cap) return AMICA_ERR_INVALIDPARAM;
     c->nclusters = ncl;
-    c->nslots = ncl * (c->use_tc ? tc_partial_groups(c->n) : plain_partial_groups(c->n));
+    c->nslots = ncl * (c->use_tc ? tc_partial_groups(c->n) : c->use_split ? 1 : plain_partial_groups(c->n));
     if (c->graph) {
         CK(cudaStreamSynchronize(c->st));
         cudaGraphExecDestroy(c->graph);
@@ -760,8 +852,14 @@ int amica_loglik_adjoint(amica_ctx* c, double* ll, double* dW, double* dmu, doub
     if (!c->d_grad) CK(cudaMalloc(&c->d_grad, sizeof(double) * glen));
     CK(launch_prep(c->b, c->hc, c->st));
     EStepArgs a = estep_args(c);
-    CK(launch_adjoint(a, c->NP, c->b.partial, c->nclusters, c->st, c->use_tc));
-    CK(launch_adjoint_finalize(c->b.partial, c->b.raw, c->nslots, n, m, M, c->b.A, c->b.c,
+    int ncl = c->nclusters, nsl = c->nslots;
+    if (c->use_split) {                           // the plain gradient kernel, on its own grid
+        ncl = c->adj_nclusters;
+        nsl = ncl * plain_partial_groups(n);
+        a.nclusters = ncl;
+    }
+    CK(launch_adjoint(a, c->NP, c->b.partial, ncl, c->st, c->use_tc));
+    CK(launch_adjoint_finalize(c->b.partial, c->b.raw, nsl, n, m, M, c->b.A, c->b.c,
                                c->b.beta, c->b.rho, c->d_grad, c->hc.psi_is_phi, c->st));
     TRY(check_device_error(c));
     std::vector<double> g(glen);
@@ -903,11 +1001,14 @@ int amica_time_estep(amica_ctx* c, int64_t reps, double* ms_per_launch, int64_t*
     CK(launch_prep(c->b, c->hc, c->st));
     EStepArgs a = estep_args(c);
     // one untimed launch, then reps timed back-to-back launches of the fused kernel
-    if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st));
+    // (the split form: its whole E-step, GEMMs included)
+    if (c->use_split) TRY(enqueue_split_estep(c, a));
+    else if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st));
     else CK(launch_estep_plain(a, c->NP, c->nclusters, c->st));
     CK(cudaEventRecord(c->ev0, c->st));
     for (int64_t r = 0; r < reps; r++) {
-        if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st));
+        if (c->use_split) TRY(enqueue_split_estep(c, a));
+        else if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st));
         else CK(launch_estep_plain(a, c->NP, c->nclusters, c->st));
     }
     CK(cudaEventRecord(c->ev1, c->st));
@@ -916,7 +1017,10 @@ int amica_time_estep(amica_ctx* c, int64_t reps, double* ms_per_launch, int64_t*
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     *ms_per_launch = (double)ms / (double)reps;
-    if (launches) *launches = reps + 2;
+    // the constants' kernels, then (reps + 1) E-steps: the split form's E-step
+    // is the W split, the kernel and one Psi add per sample chunk
+    const int64_t per = c->use_split ? 2 + (c->T + kPsiChunk - 1) / kPsiChunk : 1;
+    if (launches) *launches = (reps + 1) * per + 1;
     return AMICA_OK;
 }
 

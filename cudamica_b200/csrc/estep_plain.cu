@@ -15,8 +15,16 @@
 //      src/amica.cu:1535-1550, with phi formed from Psi in the FP64 M-step).
 // Partial sums go to a per-CTA slot of `partial`; a separate kernel reduces
 // the slots in a fixed order, so results are deterministic.
+//
+// Density-only form (EXT): the two contractions run outside the kernel as
+// TF32 tensor-core GEMMs (b = W x before it, Psi = sum g x^T after it), and
+// the kernel reads its b tile from that GEMM's output and writes g per
+// sample.  One CTA then holds all NP channels of its model, so a cluster is
+// the M models of a tile stream.
 #include <cooperative_groups.h>
 #include <cstdio>
+
+#include <algorithm>
 
 #include "common.cuh"
 #include "density.cuh"
@@ -33,9 +41,9 @@ constexpr int kS = 64;  // samples per tile
 // model holds them all; at 256 the Q = 4 CTAs of a model each own NPL = 64
 // channels (their rows of W, their densities, their rows of Psi) and read the
 // full x tile; their per-sample channel sums are added in the cluster.
-template <int NP>
+template <int NP, bool EXT = false>
 struct PlainShape {
-    static constexpr int NPL = NP <= 128 ? NP : 64; // channels of this CTA
+    static constexpr int NPL = (EXT || NP <= 128) ? NP : 64; // channels of this CTA
     static constexpr int Q = NP / NPL;              // CTAs per model
     static constexpr int SPLIT = kThreads / NPL;    // sample groups per channel
     static constexpr int SUB = kS / SPLIT;          // samples per thread per tile
@@ -49,20 +57,22 @@ struct PlainShape {
     static constexpr int RI = NPL / 16;
     static constexpr int RK = NP / 16;
     static constexpr int LLD = NPL + 1;             // padded row of the lse tile
-    static constexpr size_t smem_floats = (size_t)NP * WLD + (size_t)kS * XLD + (size_t)kS * NPL +
-                                          (size_t)kS * LLD + (size_t)kS * LLD + 2 * kS + 2 * kS;
+    static constexpr size_t smem_floats =
+        EXT ? (size_t)kS * NPL + (size_t)kS * LLD + 2 * kS + 2 * kS
+            : (size_t)NP * WLD + (size_t)kS * XLD + (size_t)kS * NPL + (size_t)kS * LLD +
+                  (size_t)kS * LLD + 2 * kS + 2 * kS;
 };
 
-template <int NP, int MM>
+template <int NP, int MM, bool EXT>
 __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
-    using Sh = PlainShape<NP>;
+    using Sh = PlainShape<NP, EXT>;
     constexpr int NPL = Sh::NPL, Q = Sh::Q;
     extern __shared__ __align__(16) float sm[];
     float* Wt = sm;                                   // [NP][WLD]  Wt[k][i] = W[i0 + i][k]
-    float* xs = Wt + NP * Sh::WLD;                    // [S][XLD]
-    float* bs = xs + kS * Sh::XLD;                    // [S][NPL]   (W x)_i per sample
+    float* xs = EXT ? sm : Wt + NP * Sh::WLD;         // [S][XLD]
+    float* bs = EXT ? sm : xs + kS * Sh::XLD;         // [S][NPL]   (W x)_i per sample
     float* gs = bs + kS * NPL;                        // [S][NPL] g; its region is [S][LLD]
-    float* lse = gs + kS * Sh::LLD;                   // [S][LLD]   log-sum-exp over mixtures
+    float* lse = EXT ? gs : gs + kS * Sh::LLD;        // [S][LLD]   log-sum-exp over mixtures
     float* slot = lse + kS * Sh::LLD;                 // [2][S]     cluster-visible L_h(t)
     float* vS = slot + 2 * kS;                        // [S]        v_h(t) (0 if not used)
 
@@ -78,10 +88,12 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     }
 
     // ---- resident per-CTA data: W_h^T and this thread's mixture constants
-    const float* Wh = a.Wf + ((size_t)h * NP + i0c) * NP;
-    for (int e = tid; e < NPL * NP; e += kThreads) {
-        int i = e / NP, k = e % NP;
-        Wt[k * Sh::WLD + i] = Wh[e];
+    if constexpr (!EXT) {
+        const float* Wh = a.Wf + ((size_t)h * NP + i0c) * NP;
+        for (int e = tid; e < NPL * NP; e += kThreads) {
+            int i = e / NP, k = e % NP;
+            Wt[k * Sh::WLD + i] = Wh[e];
+        }
     }
     const int ch = tid % NPL;           // density-phase channel (of this CTA)
     const int grp = tid / NPL;          // density-phase sample group
@@ -123,15 +135,26 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
         for (int j = 0; j < MM; j++) dA[k][j] = 0.0;
     double dCn = 0.0, dS2 = 0.0, dGs = 0.0;
     double dLL = 0.0, dVs = 0.0;   // per-sample threads (tid < S)
-    float psi[Sh::RI][Sh::RK];
+    constexpr int PRI = EXT ? 1 : Sh::RI, PRK = EXT ? 1 : Sh::RK;
+    float psi[PRI][PRK];
 #pragma unroll
-    for (int r = 0; r < Sh::RI; r++)
+    for (int r = 0; r < PRI; r++)
 #pragma unroll
-        for (int c = 0; c < Sh::RK; c++) psi[r][c] = 0.f;
+        for (int c = 0; c < PRK; c++) psi[r][c] = 0.f;
 
     int par = 0;
     for (int tile = cid; tile < a.ntiles; tile += a.nclusters, par ^= 1) {
         const int64_t t0 = (int64_t)tile * kS;
+        if constexpr (EXT) {
+            // ---- the b tile of this model from the GEMM output (samples past T are zero)
+            const float* bsrc = a.bext + (size_t)h * NP + i0c;
+            for (int e = tid; e < kS * (NPL / 4); e += kThreads) {
+                const int t = e / (NPL / 4), i4 = e % (NPL / 4);
+                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (t0 + t < a.T) v = reinterpret_cast<const float4*>(bsrc + (t0 + t) * a.ldb)[i4];
+                *reinterpret_cast<float4*>(bs + t * NPL + 4 * i4) = v;
+            }
+        } else {
         // ---- stage the x tile (float4, coalesced; rows past T are zero)
         for (int e = tid; e < kS * (NP / 4); e += kThreads) {
             int t = e / (NP / 4), k4 = e % (NP / 4);
@@ -171,6 +194,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
             for (int c = 0; c < Sh::CT; c++)
                 *reinterpret_cast<float4*>(bs + (tt * Sh::CT + c) * NPL + 4 * ti) =
                     make_float4(acc[c][0], acc[c][1], acc[c][2], acc[c][3]);
+        }
         }
         __syncthreads();
         // ---- phase 1: per (channel, sample) log-sum-exp over mixtures (log2 units)
@@ -272,7 +296,13 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
                 fCn = fmaf(v, bb, fCn);          // sum v b; cnew = A sum(v b) / vsum + c
                 fS2 = fmaf(v * bb, bb, fS2);
                 fGs += ch_ok ? g : 0.f;
-                gs[t * NPL + ch] = ch_ok ? g : 0.f;
+                if constexpr (EXT) {
+                    // stored as TF32 (round to nearest, ties away) so that the Psi GEMM reads it exactly
+                    const float gt = __uint_as_float((__float_as_uint(g) + 0x1000u) & 0xffffe000u);
+                    if (t0 + t < a.T) a.gout[(size_t)(t0 + t) * a.ldb + (size_t)h * NP + i0c + ch] = ch_ok ? gt : 0.f;
+                } else {
+                    gs[t * NPL + ch] = ch_ok ? g : 0.f;
+                }
             }
             if (ch_ok) {
 #pragma unroll
@@ -289,7 +319,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
         }
         __syncthreads();
         // ---- Psi_h += g x^T over the tile (thread: RI x RK block)
-        {
+        if constexpr (!EXT) {
             const int pi = tid % 16, pk = tid / 16;
             const int i0 = pi * Sh::RI, k0 = pk * Sh::RK;
 #pragma unroll 4
@@ -312,7 +342,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     PartLayout L{n, MM};
     // one slot per (cluster, channel block); entries of the other blocks stay zero
     double* out = a.partial + ((size_t)(cid * Q + cq) * M + h) * L.stride();
-    double* red = reinterpret_cast<double*>(xs);   // [SPLIT][NPL] doubles, one statistic at a time
+    double* red = reinterpret_cast<double*>(EXT ? bs : xs);   // [SPLIT][NPL] doubles, one statistic at a time
     constexpr int NACC = 7 * MM + 3;
     double vals[NACC];
 #pragma unroll
@@ -350,7 +380,10 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
         out[0] = s0;
         out[1] = s1;
     }
-    {
+    if constexpr (EXT) {
+        // Psi is summed by the GEMM after this kernel into the first slot
+        for (int e = tid; e < n * n; e += kThreads) out[L.psi() + e] = 0.0;
+    } else {
         const int pi = tid % 16, pk = tid / 16;
         const int i0 = pi * Sh::RI, k0 = pk * Sh::RK;
 #pragma unroll
@@ -365,11 +398,11 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     cluster.sync();
 }
 
-template <int NP, int MM>
+template <int NP, int MM, bool EXT = false>
 cudaError_t launch_plain(const EStepArgs& a, int nclusters, cudaStream_t st) {
-    using Sh = PlainShape<NP>;
+    using Sh = PlainShape<NP, EXT>;
     const size_t smem = Sh::smem_floats * sizeof(float);
-    auto kern = estep_plain_kernel<NP, MM>;
+    auto kern = estep_plain_kernel<NP, MM, EXT>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     if (a.M * Sh::Q > 1) {
@@ -405,11 +438,11 @@ int plain_partial_groups(int n) { return plain_pad_channels(n) == 256 ? PlainSha
 
 // Largest cluster count whose clusters can all be resident at once (the grid
 // is persistent: every cluster loops over its share of the tiles).
-template <int NP, int MM>
+template <int NP, int MM, bool EXT = false>
 int max_active_clusters(int M) {
-    using Sh = PlainShape<NP>;
+    using Sh = PlainShape<NP, EXT>;
     const size_t smem = Sh::smem_floats * sizeof(float);
-    auto kern = estep_plain_kernel<NP, MM>;
+    auto kern = estep_plain_kernel<NP, MM, EXT>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return -1;
     const int csize = M * Sh::Q;
@@ -465,6 +498,71 @@ cudaError_t launch_estep_plain(const EStepArgs& a, int NP, int nclusters, cudaSt
 #undef AMICA_PLAIN_NP
 #undef AMICA_PLAIN_CASE
     return cudaErrorInvalidValue;
+}
+
+// ---- density-only form (128 < n <= 256, mixed precision)
+bool plain_ext_supported(int n) { return plain_pad_channels(n) == 256; }
+
+int plain_ext_max_clusters(int m, int M) {
+    if (m < 1 || m > 5 || M < 1 || M > kMaxModels) return -1;
+#define AMICA_EXT_OCC(MMV) \
+    if (m == MMV) return max_active_clusters<256, MMV, true>(M);
+    AMICA_EXT_OCC(1) AMICA_EXT_OCC(2) AMICA_EXT_OCC(3) AMICA_EXT_OCC(4) AMICA_EXT_OCC(5)
+#undef AMICA_EXT_OCC
+    return -1;
+}
+
+cudaError_t launch_estep_plain_ext(const EStepArgs& a, int nclusters, cudaStream_t st) {
+    if (!a.bext || !a.gout || a.ldb < a.M * 256) return cudaErrorInvalidValue;
+#define AMICA_EXT_CASE(MMV) \
+    if (a.m == MMV) return launch_plain<256, MMV, true>(a, nclusters, st);
+    AMICA_EXT_CASE(1) AMICA_EXT_CASE(2) AMICA_EXT_CASE(3) AMICA_EXT_CASE(4) AMICA_EXT_CASE(5)
+#undef AMICA_EXT_CASE
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace amica
+
+namespace {
+
+// W_hi = tf32(W) (round to nearest, ties away: the low 13 bits zero, so the
+// GEMM's own TF32 conversion keeps it exactly) and W_lo = W - W_hi.
+__global__ void k_split_w(const float* __restrict__ Wf, float* __restrict__ whi, float* __restrict__ wlo,
+                          int64_t len) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < len; e += (int64_t)gridDim.x * blockDim.x) {
+        const float w = Wf[e];
+        float hi = w;
+        if (isfinite(w)) hi = __uint_as_float((__float_as_uint(w) + 0x1000u) & 0xffffe000u);
+        whi[e] = hi;
+        wlo[e] = w - hi;
+    }
+}
+
+// partial slot 0: Psi_h += the FP32 GEMM result of one sample chunk (n x n per model)
+__global__ void k_psi_add(const float* __restrict__ psi32, double* __restrict__ partial, int n, int M,
+                          int64_t stride, int psi_off) {
+    const int64_t nn = (int64_t)n * n;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < M * nn; e += (int64_t)gridDim.x * blockDim.x) {
+        const int h = (int)(e / nn);
+        partial[h * stride + psi_off + (e - h * nn)] += (double)psi32[e];
+    }
+}
+
+}  // namespace
+
+namespace amica {
+
+cudaError_t launch_split_w(const float* Wf, float* whi, float* wlo, int64_t len, cudaStream_t st) {
+    k_split_w<<<(int)std::min<int64_t>((len + 255) / 256, 1184), 256, 0, st>>>(Wf, whi, wlo, len);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_psi_add(const float* psi32, double* partial, int n, int m, int M, cudaStream_t st) {
+    PartLayout L{n, m};
+    const int64_t len = (int64_t)M * n * n;
+    k_psi_add<<<(int)std::min<int64_t>((len + 255) / 256, 1184), 256, 0, st>>>(psi32, partial, n, M,
+                                                                               L.stride(), L.psi());
+    return cudaGetLastError();
 }
 
 }  // namespace amica

@@ -1,13 +1,16 @@
 """128 < n <= 256 channels: the channel-split plain E-step (four CTAs per model
-in one cluster), the Gauss-Jordan inverse on a global working copy, and the
-GPU sphering (quadrant covariance, grid-wide Jacobi, sliced sphere apply),
-against the FP64 oracle and numpy.  Above 128 channels the mixed-precision
-request runs the plain FP32 E-step (the tensor-core form holds W in one SM).
+in one cluster), the split mixed form (b = W x and Psi = sum g x^T as TF32
+tensor-core GEMMs around the density-only E-step), the blocked Gauss-Jordan
+inverse on a global working copy, and the GPU sphering (quadrant covariance,
+grid-wide Jacobi, sliced sphere apply), against the FP64 oracle and numpy.
 
-Tolerances are those of tests/test_engine_gpu.py (FP32 densities and sums,
-FP64 totals): E-step sums 2e-5 relative, LL 2e-6 nats per sample and channel
-at identical parameters, x5 per iteration along a trajectory; mu_den (see
-compare_stats) through its median and the share of entries off by over 1%.
+Tolerances are those of tests/test_engine_gpu.py: for the plain form (FP32
+densities and sums, FP64 totals) E-step sums 2e-5 relative, LL 2e-6 nats per
+sample and channel at identical parameters, x5 per iteration along a
+trajectory; for the split mixed form (TF32 contractions: the data and g
+rounded to TF32, W as an exact TF32 hi part plus a rounded lo part) the
+mixed-form bounds, sums 2e-4 and LL 1e-5; mu_den (see compare_stats) through
+its median and the share of entries off by over 1%.
 """
 import numpy as np
 import pytest
@@ -18,6 +21,14 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 STAT_KEYS_TIGHT = ("vs", "cn", "s2", "us", "kn", "ln", "mn", "bd", "rn", "phi")
+
+
+def tf32(a):
+    """Round to TF32 (nearest, ties away), as the mixed forms store the data."""
+    u = np.ascontiguousarray(a, dtype=np.float32).copy().view(np.uint32)
+    u += np.uint32(0x1000)
+    u &= np.uint32(0xFFFFE000)
+    return u.view(np.float32).astype(np.float64)
 
 
 def case(n, T, M, m, seed):
@@ -35,7 +46,8 @@ def engine(n, T, M, m, xs, means, S, ldetS, A0, c0, precision=0):
     return eng
 
 
-def compare_stats(s_gpu, s_orc, n, M, m):
+def compare_stats(s_gpu, s_orc, n, M, m, tight=2e-5, md_med=1e-4, md_off=1e-2, md_share=0.02,
+                  phi_tol=None):
     a = O.split_stats(s_gpu, n, M, m)
     b = O.split_stats(s_orc, n, M, m)
     vsum = float(np.max(b["vs"]))
@@ -43,32 +55,53 @@ def compare_stats(s_gpu, s_orc, n, M, m):
     for k in STAT_KEYS_TIGHT + ("md",):
         scale = max(np.max(np.abs(b[k])), vsum if k == "cn" else 0.0)
         errs[k] = float(np.max(np.abs(a[k] - b[k])) / max(scale, 1e-300))
+    print("relative errors", errs)
     for k in STAT_KEYS_TIGHT:
-        assert errs[k] < 2e-5, (k, errs)
+        assert errs[k] < (phi_tol if k == "phi" and phi_tol else tight), (k, errs)
     # mu_den = rho sum u |y|^(rho-2) (rho <= 2) is carried by the few samples
     # with y near 0, where the FP32 b moves single entries by tens of percent
     # (the worst of the n m M entries reached 0.27 here): the test bounds its
-    # typical entry and the share of entries off by more than 1%
+    # typical entry and the share of entries off by more than md_off.  The
+    # TF32 data of the split form moves y near 0 by more (n=200, m=5: median
+    # 4e-3, 99th percentile 0.10, worst 0.26)
     rel = np.abs(a["md"] - b["md"]) / np.maximum(np.abs(b["md"]), 1e-300)
     q = np.quantile(rel, [0.5, 0.9, 0.99, 1.0])
     print("mu_den relative error quantiles 50/90/99/100%:", q)
-    assert q[0] < 1e-4, q
-    assert float(np.mean(rel > 1e-2)) < 0.02, q
+    assert q[0] < md_med, q
+    assert float(np.mean(rel > md_off)) < md_share, q
     return errs
 
 
-@pytest.mark.parametrize("n,M,m,precision", [(256, 2, 3, 0), (200, 1, 5, 1), (160, 3, 2, 0)])
+@pytest.mark.parametrize("n,M,m,precision", [(256, 2, 3, 0), (200, 1, 5, 1), (160, 3, 2, 0),
+                                               (256, 4, 5, 1), (144, 2, 3, 1)])
 def test_estep_stats_match_oracle(n, M, m, precision):
     T = 12000
     x, xs, means, S, ldetS, A0, c0 = case(n, T, M, m, seed=n + M)
     eng = engine(n, T, M, m, xs, means, S, ldetS, A0, c0, precision)
-    assert eng.kernel == "plain_fp32"
+    assert eng.kernel == ("split_tf32" if precision else "plain_fp32")
     orc = O.Oracle(xs, M, m, A0, c0, ldetS, nthreads=8, update_rho=1)
     orc.prepare()
     s_orc = orc.estep()
     s_gpu = eng.estep_stats()
-    assert abs(s_gpu[0] - s_orc[0]) / (n * T) < 2e-6
-    compare_stats(s_gpu, s_orc, n, M, m)
+    dll = abs(s_gpu[0] - s_orc[0]) / (n * T)
+    print("LL error per sample and channel", dll)
+    if precision:
+        # against the oracle on the data the GPU holds (x rounded to TF32): the
+        # contractions and densities are FP32-accurate, phi apart (g enters the
+        # Psi GEMM rounded to TF32, as in the fused mixed form: ~7e-5) ...
+        orc_t = O.Oracle(tf32(xs), M, m, A0, c0, ldetS, nthreads=8, update_rho=1)
+        orc_t.prepare()
+        s_orc_t = orc_t.estep()
+        assert abs(s_gpu[0] - s_orc_t[0]) / (n * T) < 2e-6
+        compare_stats(s_gpu, s_orc_t, n, M, m, tight=5e-5, md_med=1e-3, md_off=0.1, md_share=0.02,
+                      phi_tol=2e-4)
+        # ... and the TF32 data accounts for the rest (kappa and mu_den, whose
+        # terms grow as |y| -> 0, move most)
+        assert dll < 1e-5
+        compare_stats(s_gpu, s_orc, n, M, m, tight=5e-4, md_med=1e-2, md_off=0.1, md_share=0.05)
+    else:
+        assert dll < 2e-6
+        compare_stats(s_gpu, s_orc, n, M, m)
     # the inverse behind the E-step: W = A^{-1} per model
     prm = eng.params()
     for h in range(M):
@@ -88,6 +121,28 @@ def test_first_iterations_match_oracle():
         ll_orc = orc.step()
         assert abs(out.ll - ll_orc) < 2e-6 * 5 ** (it - 1), (it, out.ll, ll_orc)
     eng.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_first_iterations_split_form(precision):
+    """Both forms along a short trajectory from the same start: the split mixed
+    form against the oracle within the mixed-form LL bound (x5 per iteration),
+    and its graph replay identical to stepping."""
+    n, T, M, m = 256, 10000, 2, 3
+    x, xs, means, S, ldetS, A0, c0 = case(n, T, M, m, seed=21)
+    eng = engine(n, T, M, m, xs, means, S, ldetS, A0, c0, precision)
+    orc = O.Oracle(xs, M, m, A0, c0, ldetS, nthreads=8, update_rho=1)
+    outs = []
+    for it in range(1, 4):
+        out = eng.step()
+        ll_orc = orc.step()
+        tol = (1e-5 if precision else 2e-6) * 5 ** (it - 1)
+        assert abs(out.ll - ll_orc) < tol, (it, out.ll, ll_orc)
+        outs.append(out.ll)
+    eng.close()
+    eng2 = engine(n, T, M, m, xs, means, S, ldetS, A0, c0, precision)
+    assert [o.ll for o in eng2.run(3)] == outs
+    eng2.close()
 
 
 @pytest.mark.parametrize("n", [144, 256])
