@@ -74,6 +74,14 @@ struct StatLayout {
 
 enum MixStat { kUs = 0, kKn = 1, kLn = 2, kMn = 3, kMd = 4, kBd = 5, kRn = 6 };
 
+// A model whose responsibilities sum to less than one sample (vsum_h < 1: it
+// explains no data) is frozen: its A, c and mixture parameters keep their
+// values and gm_h = max(vsum_h / T, kMinGm).  The reference divides by vsum_h
+// and usum_hij regardless (src/amica.cu:1995-2154), which turns such a
+// model's parameters non-finite within a few iterations.
+constexpr double kMinModelVsum = 1.0;
+constexpr double kMinGm = 1e-300;
+
 // Everything the fused E-step kernel needs, by value.
 struct EStepArgs {
     const float* x;          // T x ldx sphered data (channels >= n are zero)

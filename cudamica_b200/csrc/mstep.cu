@@ -697,6 +697,14 @@ __global__ void __launch_bounds__(256) k_gemm64(GemmArgs g) {
     const double ivs = g.kind == 0 ? 1.0 / g.stats[SL.base(h) + SL.vs()] : 0.0;
     const double* kappa = g.kind == 0 ? g.work + (size_t)h * 4 * n : nullptr;
     const int newton = g.kind == 0 ? g.use_newton[h] : 0;
+    if (newton < 0) {                                 // frozen model: A unchanged
+        const int r = r0 + tx;
+        for (int q = 0; q < 4; q++) {
+            const int col = c0 + ty + 8 * q;
+            if (r < n && col < n) g.Out[g.strideOut * h + (size_t)col * n + r] = Xh[(size_t)col * n + r];
+        }
+        return;
+    }
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (int k0 = 0; k0 < n; k0 += 32) {
         for (int q = 0; q < 4; q++) {
@@ -746,8 +754,10 @@ __global__ void __launch_bounds__(1024) k_reparm(int update_A, int do_reparm, do
                                                  const double* __restrict__ Anew,
                                                  const double* __restrict__ W, double* c,
                                                  double* mu, double* beta,
-                                                 const double* __restrict__ work, int n, int m) {
+                                                 const double* __restrict__ work,
+                                                 const int* __restrict__ use_newton, int n, int m) {
     const int h = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (use_newton[h] < 0) return;                    // frozen model: A, c, mu, beta unchanged
     const double* cnew = work + (size_t)h * 4 * n + 3 * n;
     double* ch = c + (size_t)h * n;
     __shared__ double norms[kMaxN], shift[kMaxN], dc[kMaxN];
@@ -903,7 +913,16 @@ __global__ void __launch_bounds__(kMT) k_mstep_params(
     __shared__ double ks[kMaxN];
     const double vsum = S[SL.vs()];
     const double ivs = 1.0 / vsum;
+    if (!(vsum >= kMinModelVsum)) {                   // a model that explains no data: frozen
+        if (tid == 0) {
+            if (cf.update_gm) gm[h] = fmax(vsum / Tk, kMinGm);
+            bflag[h] = 0;
+            use_newton[h] = -1;
+        }
+        return;
+    }
     if (tid == 0 && cf.update_gm) gm[h] = vsum / Tk;
+    if (tid == 0 && !cf.update_A) use_newton[h] = 0;
     // alpha = usum / vsum; then kappa / lambda with the new alpha and old mu
     for (int i = tid; i < n; i += kMT) {
         const double s2 = S[SL.s2() + i] * ivs;
@@ -1169,7 +1188,7 @@ cudaError_t launch_mstep(const MStepBuffers& b, const MStepCfgHost& h, const flo
         k_gemm64<<<g, 256, 0, st>>>(ga);
     }
     k_reparm<<<h.M, 1024, 0, st>>>(h.update_A, h.do_reparm, b.A, b.Anew, b.W, b.c, b.mu, b.beta,
-                                  b.work, h.n, h.m);
+                                  b.work, b.use_newton, h.n, h.m);
     if (h.do_reject && P_rel && keep)
         k_reject<<<1, kT, 0, st>>>(cf, b.ctrl, P_rel, keep, T, b.chunk, b.hist, b.hist_cap, 0);
     return cudaGetLastError();

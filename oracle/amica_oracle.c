@@ -523,9 +523,20 @@ int amo_mstep(const amo_cfg *cfg, amo_state *st, const double *stats) {
     double *kappa = calloc(M * n, sizeof(double)), *lambda = calloc(M * n, sizeof(double));
     double *sig2 = malloc(sizeof(double) * M * n), *cnew = malloc(sizeof(double) * M * n);
     double *phi = malloc(sizeof(double) * M * n * n);
+    /* A model whose responsibilities sum to less than one sample explains no
+     * data: it is frozen (A, c and its mixture parameters kept, gm floored at
+     * 1e-300), where the reference's divisions by vsum and usum would make its
+     * parameters non-finite.  The GPU engine applies the same rule. */
+    int *frozen = calloc(M, sizeof(int));
     for (int64_t h = 0; h < M; h++) {
         const double *S = stats + 1 + h * o.S;
         const double vsum = S[o.vs];
+        if (!(vsum >= 1.0)) {
+            frozen[h] = 1;
+            if (cfg->update_gm) st->gm[h] = fmax(vsum / Tk, 1e-300);
+            for (int64_t i = 0; i < n; i++) cnew[h * n + i] = st->c[h * n + i];
+            continue;
+        }
         if (cfg->update_gm) st->gm[h] = vsum / Tk;                 /* :1995-2000 */
         for (int64_t mi = 0; mi < mn; mi++)                         /* alpha = usum / vsum, :2006-2023 */
             if (cfg->update_alpha) st->alpha[h * mn + mi] = S[o.us + mi] * (1.0 / vsum);
@@ -576,6 +587,7 @@ int amo_mstep(const amo_cfg *cfg, amo_state *st, const double *stats) {
         for (int64_t h = 0; h < M; h++) {
             const double *ph = phi + h * n * n;
             double *Bh = B + h * n * n;
+            if (frozen[h]) continue;
             /* denoms = (kappa sigma2)(kappa sigma2)^T; bflag counts entries <= 1
              * over the full n x n grid, diagonal included (src/kernels.cu:975-979) */
             int64_t bflag = 0;
@@ -617,6 +629,7 @@ int amo_mstep(const amo_cfg *cfg, amo_state *st, const double *stats) {
         double *dc = malloc(sizeof(double) * n);
         for (int64_t h = 0; h < M; h++) {
             /* A <- A +/- lrate * A * B, src/amica.cu:2317-2342 */
+            if (frozen[h]) continue;
             double *Ah = st->A + h * n * n;
             const double *Bh = B + h * n * n;
             double al = use_newton[h] ? st->lrate : -st->lrate;
@@ -631,6 +644,7 @@ int amo_mstep(const amo_cfg *cfg, amo_state *st, const double *stats) {
         if (cfg->do_reparm) {
             for (int64_t h = 0; h < M; h++) {
                 /* normalizeAsave + normalizemubeta, src/kernels.cu:1023-1052 */
+                if (frozen[h]) continue;
                 double *Ah = st->A + h * n * n;
                 for (int64_t c = 0; c < n; c++) {
                     double s = 0.0;
@@ -648,6 +662,7 @@ int amo_mstep(const amo_cfg *cfg, amo_state *st, const double *stats) {
             for (int64_t h = 0; h < M; h++) {
                 /* cnewminusc + W (cnew - c) + substract, src/amica.cu:2402-2437,
                  * with W from the start of the iteration */
+                if (frozen[h]) continue;
                 const double *Wh = st->W + h * n * n;
                 for (int64_t k = 0; k < n; k++) dc[k] = cnew[h * n + k] - st->c[h * n + k];
                 for (int64_t i = 0; i < n; i++) {
@@ -662,7 +677,7 @@ int amo_mstep(const amo_cfg *cfg, amo_state *st, const double *stats) {
     /* c <- cnew, src/amica.cu:2456-2462 */
     memcpy(st->c, cnew, sizeof(double) * M * n);
     st->iter = iter;
-    free(kappa); free(lambda); free(sig2); free(cnew); free(phi);
+    free(kappa); free(lambda); free(sig2); free(cnew); free(phi); free(frozen);
     return 0;
 }
 
