@@ -16,6 +16,7 @@ enum : int {
     kErrWaitTimeout = 1,      // a bounded mbarrier / flag wait gave up
     kErrShape = 2,            // launch received a shape it was not built for
     kErrSingular = 4,         // zero pivot while inverting A
+    kErrNonFinite = 8,        // the M-step produced a non-finite parameter
 };
 
 // Per-(model, mixture, channel) E-step constants, derived in FP64 from the
@@ -76,9 +77,12 @@ enum MixStat { kUs = 0, kKn = 1, kLn = 2, kMn = 3, kMd = 4, kBd = 5, kRn = 6 };
 
 // A model whose responsibilities sum to less than one sample (vsum_h < 1: it
 // explains no data) is frozen: its A, c and mixture parameters keep their
-// values and gm_h = max(vsum_h / T, kMinGm).  The reference divides by vsum_h
-// and usum_hij regardless (src/amica.cu:1995-2154), which turns such a
-// model's parameters non-finite within a few iterations.
+// values and gm_h = max(vsum_h / T, kMinGm).  Likewise a mixture component
+// with no responsibility at all (usum_hij = 0: every FP32 responsibility
+// underflowed) keeps its mu, beta and rho and drops out of the kappa and
+// lambda sums (its alpha is 0).  The reference divides by vsum_h and usum_hij
+// regardless (src/amica.cu:1995-2154), which turns such parameters, and
+// through kappa/lambda and the A update the whole model, non-finite.
 constexpr double kMinModelVsum = 1.0;
 constexpr double kMinGm = 1e-300;
 

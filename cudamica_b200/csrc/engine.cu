@@ -263,12 +263,12 @@ int enqueue_estep(amica_ctx* c) {
 
 // Kernels one iteration launches: inverse/derive, E-step, reduce, finalize
 // (+ phi from Psi in the plain form), params, ctrl, A update (when A is
-// updated), reparametrisation (+ rejection when enabled).
+// updated), reparametrisation, the finiteness check (+ rejection when enabled).
 int launches_per_iteration(const amica_ctx* c) {
     // the split form adds the W split and one Psi add per sample chunk (its
     // GEMMs are library kernels and not counted)
     const int split = c->use_split ? 1 + (int)((c->T + kPsiChunk - 1) / kPsiChunk) : 0;
-    return 7 + split + (c->hc.psi_is_phi ? 0 : 1) + (c->hc.update_A ? 1 : 0) + (c->hc.do_reject ? 1 : 0);
+    return 8 + split + (c->hc.psi_is_phi ? 0 : 1) + (c->hc.update_A ? 1 : 0) + (c->hc.do_reject ? 1 : 0);
 }
 
 int enqueue_iteration(amica_ctx* c) {
@@ -286,6 +286,7 @@ int check_device_error(amica_ctx* c) {
         if (e & kErrWaitTimeout) return AMICA_ERR_TIMEOUT;
         if (e & kErrSingular) return AMICA_ERR_SINGULAR;
         if (e & kErrShape) return AMICA_ERR_UNSUPPORTED;
+        if (e & kErrNonFinite) return AMICA_ERR_NUMERIC;
         return AMICA_ERR_CUDA;
     }
     return AMICA_OK;

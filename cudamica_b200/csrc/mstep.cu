@@ -7,6 +7,7 @@
 // host SVD for pinv, a synchronous bflag copy, ...).  Here it is six small
 // kernels that stay on the device, so that a whole iteration can be captured
 // in one CUDA graph and no host synchronisation is needed between iterations.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 
@@ -934,6 +935,7 @@ __global__ void __launch_bounds__(kMT) k_mstep_params(
             const size_t idx = (size_t)h * mn + mi;
             const double us = S[SL.mix(kUs) + mi];
             if (cf.update_alpha) alpha[idx] = us * ivs;
+            if (!(us > 0.0)) continue;                // a component with no responsibility
             const double dk = S[SL.mix(kKn) + mi] / us;
             const double a = alpha[idx];
             kap += dk * a;
@@ -947,6 +949,7 @@ __global__ void __launch_bounds__(kMT) k_mstep_params(
     __syncthreads();
     for (int mi = tid; mi < mn; mi += kMT) {
         const size_t idx = (size_t)h * mn + mi;
+        if (!(S[SL.mix(kUs) + mi] > 0.0)) continue;  // no responsibility: mu, beta, rho kept
         if (cf.update_mu) mu[idx] += S[SL.mix(kMn) + mi] / S[SL.mix(kMd) + mi];
         if (cf.update_beta) {
             const double bnum = (rho[idx] > 2.0) ? 0.0 : S[SL.mix(kUs) + mi];
@@ -1171,6 +1174,24 @@ cudaError_t launch_reduce_finalize(const MStepBuffers& b, const MStepCfgHost& h,
     return cudaGetLastError();
 }
 
+// Flags a non-finite parameter after the M-step, so that the host rolls the
+// iteration back (the next E-step would otherwise carry NaN into the LL).
+__global__ void k_check_finite(const double* __restrict__ A, const double* __restrict__ c,
+                               const double* __restrict__ alpha, const double* __restrict__ mu,
+                               const double* __restrict__ beta, const double* __restrict__ rho,
+                               const double* __restrict__ gm, int64_t nA, int64_t nc, int64_t nmix,
+                               int M, int* err) {
+    bool bad = false;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (int64_t e = t0; e < nA; e += stride) bad |= !isfinite(A[e]);
+    for (int64_t e = t0; e < nc; e += stride) bad |= !isfinite(c[e]);
+    for (int64_t e = t0; e < nmix; e += stride)
+        bad |= !isfinite(alpha[e]) || !isfinite(mu[e]) || !isfinite(beta[e]) || !isfinite(rho[e]);
+    for (int64_t e = t0; e < M; e += stride) bad |= !isfinite(gm[e]);
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(err, kErrNonFinite);
+}
+
 cudaError_t launch_mstep(const MStepBuffers& b, const MStepCfgHost& h, const float* P_rel,
                          uint8_t* keep, int64_t T, cudaStream_t st) {
     const MCfg cf = to_mcfg(h);
@@ -1189,6 +1210,12 @@ cudaError_t launch_mstep(const MStepBuffers& b, const MStepCfgHost& h, const flo
     }
     k_reparm<<<h.M, 1024, 0, st>>>(h.update_A, h.do_reparm, b.A, b.Anew, b.W, b.c, b.mu, b.beta,
                                   b.work, b.use_newton, h.n, h.m);
+    {
+        const int64_t nA = (int64_t)h.M * h.n * h.n, nmix = (int64_t)h.M * h.m * h.n;
+        const int grid = (int)std::min<int64_t>((nA + 255) / 256, 148);
+        k_check_finite<<<grid, 256, 0, st>>>(b.A, b.c, b.alpha, b.mu, b.beta, b.rho, b.gm, nA,
+                                             (int64_t)h.M * h.n, nmix, h.M, b.err);
+    }
     if (h.do_reject && P_rel && keep)
         k_reject<<<1, kT, 0, st>>>(cf, b.ctrl, P_rel, keep, T, b.chunk, b.hist, b.hist_cap, 0);
     return cudaGetLastError();

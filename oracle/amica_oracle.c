@@ -550,14 +550,20 @@ int amo_mstep(const amo_cfg *cfg, amo_state *st, const double *stats) {
             for (int64_t i = 0; i < n; i++) {
                 int64_t mi = j * n + i, idx = h * mn + mi;
                 double us = S[o.us + mi];
+                if (!(us > 0.0)) continue;    /* a component with no responsibility (see below) */
                 double dk = S[o.kn + mi] / us;
                 double a = st->alpha[idx];
                 kappa[h * n + i] += dk * a;
                 double muv = st->mu[idx];
                 lambda[h * n + i] += (muv * muv * dk + S[o.ln + mi] / us) * a;
             }
+        /* A mixture component with no responsibility at all (usum = 0) keeps its
+         * mu, beta and rho and is left out of kappa and lambda (its alpha is 0),
+         * where the reference's 0/0 would make the model non-finite; the GPU
+         * engine applies the same rule. */
         for (int64_t mi = 0; mi < mn; mi++) {
             int64_t idx = h * mn + mi;
+            if (!(S[o.us + mi] > 0.0)) continue;
             if (cfg->update_mu)                                     /* divide + acumulate, :2095-2115 */
                 st->mu[idx] += S[o.mn + mi] / S[o.md + mi];
             if (cfg->update_beta) {                                 /* getbetanumer + divide + multiply */
@@ -568,6 +574,7 @@ int amo_mstep(const amo_cfg *cfg, amo_state *st, const double *stats) {
         if (cfg->update_rho && iter >= cfg->rho_start_iter) {       /* updaterho, src/kernels.cu:937-954 */
             for (int64_t mi = 0; mi < mn; mi++) {
                 int64_t idx = h * mn + mi;
+                if (!(S[o.us + mi] > 0.0)) continue;
                 double r = st->rho[idx];
                 double ps = amo_psi(1.0 + 1.0 / r);
                 double d = 1.0 - (r / ps) * S[o.rn + mi] / S[o.us + mi];
