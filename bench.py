@@ -157,7 +157,8 @@ def traffic_per_launch():
 
 
 def time_form(x, A0, c0, precision, device, steps, warmup, fit_iters):
-    """Returns (ms per timed step, final LL after fit_iters, estep ms, kernel, launches)."""
+    """Returns (ms per timed step, final LL after fit_iters, estep ms, kernel, launches,
+    clusters): clusters is the E-step grid, as many as the device can hold at once."""
     eng = new_engine(x, A0, c0, precision, device)
     eng.run(warmup)
     outs = eng.run(steps)                     # device time via CUDA events on the engine stream
@@ -171,8 +172,9 @@ def time_form(x, A0, c0, precision, device, steps, warmup, fit_iters):
     est_ms, _ = eng.time_estep(5)
     kernel = eng.kernel
     lpi = eng.launches_per_iteration
+    grid = eng.set_grid(0)
     eng.close()
-    return ms, final_ll, est_ms, kernel, lpi
+    return ms, final_ll, est_ms, kernel, lpi, grid
 
 
 def cpu_baseline_port(x, A0, c0, sample_T: int = 100_000):
@@ -446,17 +448,17 @@ def main():
         pg.barrier()
     torch.cuda.synchronize()
     with Clocks(device) as clk:
-        t_mixed, ll_mixed, est_mixed, kname, lpi = time_form(x, A0, c0, 1, device, args.steps,
-                                                             args.warmup, args.fit_iters)
+        t_mixed, ll_mixed, est_mixed, kname, lpi, grid_mixed = time_form(x, A0, c0, 1, device, args.steps,
+                                                                         args.warmup, args.fit_iters)
     clocks = clk.summary()
-    t_plain, ll_plain, est_plain, kname_plain, _ = time_form(x, A0, c0, 0, device, args.steps,
-                                                             args.warmup, args.fit_iters)
+    t_plain, ll_plain, est_plain, kname_plain, _, grid_plain = time_form(x, A0, c0, 0, device, args.steps,
+                                                                         args.warmup, args.fit_iters)
     # control: the plain form again from A0 perturbed by 1e-12 (relative); the
     # EM map separates nearby trajectories, and this run shows by how much the
     # final LL moves for reasons that have nothing to do with precision
     rng = np.random.default_rng(123)
     A0p = A0 * (1.0 + 1e-12 * rng.standard_normal(A0.shape))
-    _, ll_ctrl, _, _, _ = time_form(x, A0p, c0, 0, device, 1, 0, args.fit_iters)
+    _, ll_ctrl, _, _, _, _ = time_form(x, A0p, c0, 0, device, 1, 0, args.fit_iters)
     ms, t_plain = reduce_over_ranks([t_mixed, t_plain], pg, "max")
     value = whole_job_rate(ms, ws)
     hbm, bf16, src = peaks()
@@ -482,9 +484,10 @@ def main():
         "config": {"workload": "n=128 T=1e6 M=3 m=3, one EM iteration per step", **WORKLOAD,
                    "precision": "mixed: tcgen05 TF32 contractions, FP32 densities, FP64 M-step",
                    "kernel": kname, "l2": "inputs larger than L2 (512 MB sphered data per step)",
-                   "parallelism": "replicas" if ws > 1 else "single GPU"},
+                   "parallelism": "replicas" if ws > 1 else "single GPU",
+                   "estep_clusters": grid_mixed},
         "plain_fp32": {"value": whole_job_rate(t_plain, ws), "ms_per_step": t_plain, "kernel": kname_plain,
-                       "estep_ms": est_plain},
+                       "estep_ms": est_plain, "estep_clusters": grid_plain},
         "mixed_over_plain": t_plain / ms,
         "final_ll": {"iters": args.fit_iters, "mixed": ll_mixed, "plain": ll_plain,
                      "abs_diff": abs(ll_mixed - ll_plain), "plain_perturbed_1e-12": ll_ctrl,
