@@ -70,3 +70,30 @@ def test_engine_freezes_a_model_without_data(precision):
     assert np.array_equal(p["A"][1], A0[1])
     assert np.array_equal(p["c"][1], c0[1])
     eng.close()
+
+
+def test_oracle_keeps_a_component_without_responsibility():
+    """alpha = 0 for one mixture component of one model: its log-density is
+    -inf, its responsibilities and usum are 0, and its mu, beta and rho get no
+    update (mu and beta still follow the reparametrisation of their channel,
+    the column scaling of A and the shift of c) while the other components
+    and the model are updated; the reference's 0/0 would have made kappa,
+    lambda and then A non-finite."""
+    d = synth.config0(seed=6, n=N, T=T)
+    xs, means, S, ldetS = O.preprocess(d.x, 1)
+    A0, c0 = synth.norand_init(N, 1)
+    # Newton from the first iteration, so that kappa and lambda enter the A update
+    orc = O.Oracle(xs, 1, MIX, A0, c0, ldetS, nthreads=4, newt_start_iter=1)
+    orc.alpha[0, 1, 3] = 0.0                  # shared with the oracle's state
+    p0 = orc.params()
+    lls = [orc.step() for _ in range(5)]
+    p = orc.params()
+    assert np.all(np.isfinite(lls)) and lls[-1] > lls[0]
+    for k, v in p.items():
+        assert np.all(np.isfinite(v)), k
+    assert p["rho"][0, 1, 3] == p0["rho"][0, 1, 3]
+    for k in ("mu", "beta", "rho"):
+        assert p[k][0, 0, 3] != p0[k][0, 0, 3], k
+    assert p["alpha"][0, 1, 3] == 0.0
+    assert not np.array_equal(p["A"], p0["A"])
+    assert orc.st.newton == 1                 # the Newton step ran
