@@ -349,6 +349,54 @@ def cohort_arm(args):
     }
 
 
+def big_arm(args):
+    """The 256-channel multi-model workload (synth.config4, seed 0: n=256,
+    T=2,000,000, M=4, m=5): the split mixed form (TF32 tensor-core GEMMs around
+    the density-only E-step) against plain FP32.  Device time per
+    graph-captured iteration (CUDA events on the engine's stream), the E-step
+    alone, and the LL of both forms after --big-fit-iters iterations from the
+    same start (or the error that stopped a fit)."""
+    from cudamica_b200 import synth
+    from cudamica_b200.engine import Amica, AmicaError
+    n, M, m = 256, 4, 5
+    T = args.big_T
+    x = np.ascontiguousarray(synth.config4(seed=0, n=n, T=T, M=M, m=m).x)
+    A0, c0 = synth.norand_init(n, M)
+    res = {}
+    for precision in (1, 0):
+        eng = Amica(n, T, M, m, precision=precision, maxiter=max(4000, args.big_fit_iters + 16))
+        eng.load_data(x)
+        eng.preprocess()
+        eng.init(A0, c0)
+        eng.run(args.warmup)
+        outs = eng.run(args.steps)
+        ms = float(np.mean([o.device_ms for o in outs]))
+        ll, status = outs[-1].ll, "ok"
+        rest = args.big_fit_iters - args.warmup - args.steps
+        try:
+            if rest > 0:
+                ll = eng.run(rest)[-1].ll
+        except AmicaError as e:
+            status = str(e)
+        est_ms, _ = eng.time_estep(3)
+        res[eng.kernel] = {"ms_per_step": ms, "value": 1000.0 / ms, "estep_ms": est_ms,
+                           "ll": ll, "fit_status": status}
+        eng.close()
+    sp, pl = res["split_tf32"], res["plain_fp32"]
+    return {
+        "metric": "EM iters/s at n=256,T=2M,M=4,m=5: split mixed form vs plain FP32",
+        "value": sp["value"], "unit": "iters/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sp["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"n=256 T={T} M=4 m=5 (synth.config4), one EM iteration per step",
+                   "n": n, "T": T, "M": M, "m": m, "kernel": "split_tf32",
+                   "precision": "mixed: TF32 tensor-core GEMMs for b = W x and Psi, FP32 densities, "
+                                "FP64 M-step", "parallelism": "single GPU"},
+        "split_tf32": sp, "plain_fp32": pl, "split_over_plain": pl["ms_per_step"] / sp["ms_per_step"],
+        "fit_iters": args.big_fit_iters,
+    }
+
+
 def profile_case(args):
     """A few E-step launches per form on the first T samples of the workload
     (or, with --profile-shape n,M,m, of the large multi-model recipe at that
@@ -395,11 +443,18 @@ def main():
     ap.add_argument("--cohort-subjects", type=int, default=48)
     ap.add_argument("--cohort-scale", type=float, default=1.0,
                     help="scale of the per-subject sample counts")
+    ap.add_argument("--big", action="store_true",
+                    help="the 256-channel workload (n=256, M=4, m=5), both forms")
+    ap.add_argument("--big-T", type=int, default=2_000_000)
+    ap.add_argument("--big-fit-iters", type=int, default=300)
     args = ap.parse_args()
     if args.profile_case:
         return profile_case(args)
     if args.cohort:
         print(json.dumps(cohort_arm(args)))
+        return 0
+    if args.big:
+        print(json.dumps(big_arm(args)))
         return 0
     ws, rank, local = dist_env()
     pg = None
