@@ -3,7 +3,7 @@
 fixtures (tests/golden/ref_<case>.npz).
 
 Needs a GPU.  Usage:
-    python tests/golden/make_ref_goldens.py --out gpurun_out/golden c0 m2 m3
+    python tests/golden/make_ref_goldens.py --out DIR c0 m2 m3
     python tests/golden/make_ref_goldens.py --time-only --out DIR c1t c2t
 
 The reference runs in its deterministic mode (-DNORAND -DITERTEST): it reads the
