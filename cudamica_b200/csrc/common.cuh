@@ -128,8 +128,8 @@ struct MStepBuffers {
     double *A, *Anew, *c, *alpha, *mu, *beta, *rho, *gm, *W, *ldet, *ltc64;
     double *partial, *raw, *stats, *work, *chunk;
     double* gj;        // n > 128: M n^2 working matrices + M n pivot logs of the inverse
-    int64_t* bflag;
-    int* use_newton;
+    int64_t* bflag;          // M: Newton-condition violations of the last M-step
+    int* use_newton;         // M: 1 Newton step, 0 natural gradient, -1 frozen model (no update)
     float *Wf, *wcf;
     MixParam* mp;
     Ctrl* ctrl;
