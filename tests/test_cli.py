@@ -97,6 +97,22 @@ def test_missing_required_key(cli, tmp_path):
     assert r.returncode != 0 and "data file" in r.stderr
 
 
+def test_truncated_data_file_is_reported(cli, tmp_path):
+    # fewer than nsamples x nchannels float32 values: an error before any GPU work
+    np.zeros((63, 4), dtype=np.float32).tofile(os.path.join(tmp_path, "data.fdt"))
+    r = run(cli, tmp_path, "\n".join(BASE) + "\n")
+    assert r.returncode == 256 - 5, (r.returncode, r.stderr)    # AMICA_ERR_NOFILE
+    assert "cannot read 64 x 4 float32 values" in r.stderr
+
+
+def test_truncated_initial_state_file_is_reported(cli, tmp_path):
+    # ainitfile shorter than one n x n block
+    small_data(tmp_path)
+    np.zeros(15, dtype=np.float32).tofile(os.path.join(tmp_path, "a0.fdt"))
+    r = run(cli, tmp_path, "\n".join(BASE + ["ainitfile a0.fdt"]) + "\n")
+    assert r.returncode == 256 - 5, (r.returncode, r.stderr)
+
+
 @pytest.mark.gpu
 def test_cli_fit_matches_reference_outputs(cli, tmp_path):
     case = CASES["c0"]
