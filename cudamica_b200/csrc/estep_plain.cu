@@ -53,6 +53,7 @@ struct PlainShape {
     static constexpr int NTI = NPL / 4;
     static constexpr int NTT = kThreads / NTI;
     static constexpr int CT = kS / NTT;
+    static_assert(EXT || NTI * NTT == kThreads && NTT * CT == kS, "b = W x tiling");
     // Psi update: each thread RI x RK block
     static constexpr int RI = NPL / 16;
     static constexpr int RK = NP / 16;
