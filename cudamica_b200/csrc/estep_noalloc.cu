@@ -11,7 +11,6 @@
 // the GPU (two streams, two host threads) race on it: serialise them.
 #include <cstdint>
 #include <cstring>
-#include <mutex>
 
 #include "amica_b200.h"
 #include "common.cuh"
@@ -32,27 +31,22 @@ using namespace amica;
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = 5u << 20;     // 5 MiB per device
-constexpr int kNoAllocMaxClusters = 8;                // grid of the E-step in this mode
-constexpr int kMaxDevices = 64;
+constexpr int kNoAllocMaxClusters = 8;                // largest E-step grid in this mode
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_setup_mutex;
-void* g_scratch_ptr[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device, resolved once per
-// device (the host-side symbol is only a handle, never a device address).
-int scratch_for_current_device(unsigned char** out) {
+// Device address of the scratch array in the CUDA context current on the
+// calling thread.  The host-side symbol is only a handle, never a device
+// address.  The lookup is repeated on every call (it is a table lookup once
+// the module is loaded) rather than cached, so that an address never outlives
+// its context: a device reset, or a caller that makes its own (non-primary)
+// context current, gets the address that is valid in that context.
+int scratch_in_current_context(unsigned char** out) {
     int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return AMICA_ERR_NODEVICE;
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr)
-            return AMICA_ERR_CUDA;
-        g_scratch_ptr[dev] = p;
-    }
-    *out = (unsigned char*)g_scratch_ptr[dev];
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return AMICA_ERR_NODEVICE;
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) return AMICA_ERR_CUDA;
+    *out = (unsigned char*)p;
     return AMICA_OK;
 }
 
@@ -100,6 +94,7 @@ extern "C" int amica_estep_stats_noalloc(const float* x, int64_t ldx, int64_t n,
     const int NP = plain_pad_channels((int)n);
     if (NP < 0 || ldx != NP) return AMICA_ERR_INVALIDPARAM;
     if (nkeep < 1 || nkeep > T) return AMICA_ERR_INVALIDPARAM;
+    if (keep == nullptr && nkeep != T) return AMICA_ERR_INVALIDPARAM;   // every sample counts
     const int ntiles = (int)((T + plain_tile_samples() - 1) / plain_tile_samples());
     int ncl = plain_max_clusters((int)n, (int)m, (int)M);
     if (ncl <= 0) return AMICA_ERR_UNSUPPORTED;
@@ -107,11 +102,15 @@ extern "C" int amica_estep_stats_noalloc(const float* x, int64_t ldx, int64_t n,
     if (ncl > ntiles) ncl = ntiles;
     // above 128 channels each cluster has one slot per channel block
     const int groups = plain_partial_groups((int)n);
+    // every cluster writes its own partial slots: use fewer clusters (down to
+    // one, which runs every tile) until the layout fits the fixed array
     MStepBuffers b;
-    const size_t need = carve(nullptr, (int)n, (int)M, (int)m, NP, ncl * groups, &b);
-    if (need > kNoAllocScratchBytes) return AMICA_ERR_UNSUPPORTED;   // beyond the fixed 5 MiB
+    while (ncl > 1 && carve(nullptr, (int)n, (int)M, (int)m, NP, ncl * groups, &b) > kNoAllocScratchBytes)
+        ncl--;
+    if (carve(nullptr, (int)n, (int)M, (int)m, NP, ncl * groups, &b) > kNoAllocScratchBytes)
+        return AMICA_ERR_UNSUPPORTED;   // beyond the fixed 5 MiB even with one cluster
     unsigned char* base = nullptr;
-    int rc = scratch_for_current_device(&base);
+    int rc = scratch_in_current_context(&base);
     if (rc != AMICA_OK) return rc;
     carve(base, (int)n, (int)M, (int)m, NP, ncl * groups, &b);
     b.A = const_cast<double*>(A);

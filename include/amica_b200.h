@@ -203,15 +203,18 @@ int amica_selftest_umma(int mode, int N, int K, const float *A, const float *B, 
  * All pointers are DEVICE memory owned by the caller: x is T x ldx float32
  * sphered data with ldx the channel count padded to 32, 64, 128 or 256 (padding
  * channels zero); A (M x n x n), c, alpha, mu, beta, rho, gm as in
- * amica_set_params(); keep (T bytes) may be NULL with nkeep = T; stats
- * receives amica_stats_len(n, M, m) doubles.  Intermediate data lives in a
- * fixed 5 MiB device array inside this library (held by every GPU that loads
- * it until exit); shapes needing more (roughly n = 128 with M > 3) return
- * AMICA_ERR_UNSUPPORTED.  The first call on a device resolves that array's
- * address for the device, so make it before any stream capture.  Calls share
- * the array: calls whose GPU work overlaps race, so serialise them.  The call
- * enqueues on `stream` (a cudaStream_t, NULL = default) and returns after
- * synchronising it. */
+ * amica_set_params(); keep (T bytes) may be NULL, and then nkeep must be T;
+ * stats receives amica_stats_len(n, M, m) doubles.  Intermediate data lives in
+ * a fixed 5 MiB device array inside this library (held by every GPU that loads
+ * it until exit).  The E-step grid shrinks, down to a single cluster, until its
+ * per-cluster partial sums fit that array; shapes that do not fit even then
+ * return AMICA_ERR_UNSUPPORTED (at n = 256 only M = 1 fits; at n = 128, M up
+ * to 8 fits).  The array's device address is looked up in the current CUDA
+ * context on every call, so device resets and caller-owned contexts are safe.
+ * Calls share the array: calls whose GPU work overlaps race, so serialise
+ * them.  The call enqueues on `stream` (a cudaStream_t, NULL = default), then
+ * copies a status word to the host and synchronises that stream; it must
+ * never be made while the stream is being captured into a CUDA graph. */
 int amica_estep_stats_noalloc(const float *x, int64_t ldx, int64_t n, int64_t T, int64_t M,
                               int64_t m, const double *A, const double *c, const double *alpha,
                               const double *mu, const double *beta, const double *rho,

@@ -77,3 +77,26 @@ def prepared(case: Case):
     xs, means, S, ldetS = sphere_numpy(x)
     A0, c0 = synth.norand_init(case.n, case.M)
     return dict(x=x, xs=xs, means=means, sphere=S, ldetS=ldetS, A0=A0, c0=c0)
+
+
+def ref_ltall_source(T: int, block_size: int, stride: int = 97, count: int | None = None):
+    """Where the reference's ltallfile entries come from.
+
+    The reference copies each block's Lt into its per-model ltall buffer at
+    ``OFFSET1D(dev_ltall, start)`` (src/amica.cu:1203-1209), and OFFSET1D adds
+    ``start`` BYTES, not elements (include/tools.h:140-141).  Block b therefore
+    lands at element b * block_size / 8, the blocks overlap (later blocks win),
+    and elements past (nblocks - 1) * block_size / 8 + block_size are never
+    written (uninitialised memory in the file).  The goldens keep every
+    ``stride``-th element of that file.
+
+    Returns (positions in the strided golden that hold a real Lt value, the
+    sample index t each of them holds)."""
+    nb = T // block_size
+    step = block_size // 8
+    n_el = -(-T // stride) if count is None else count
+    e = np.arange(n_el, dtype=np.int64) * stride
+    valid = e < (nb - 1) * step + block_size
+    blk = np.minimum(e // step, nb - 1)
+    src = blk * block_size + e - blk * step
+    return np.nonzero(valid)[0], src[valid]

@@ -76,3 +76,16 @@ def test_create_without_gpu_reports_no_device(lib):
     ctx = C.c_void_p()
     cfg = E.default_cfg(nchannels=8, nsamples=100)
     assert lib.amica_create(C.byref(cfg), C.byref(ctx)) == -26
+
+
+def test_noalloc_argument_checks(lib):
+    # argument checks come before any device call, so they hold without a GPU;
+    # dummy non-null pointers are never dereferenced on these paths
+    f = E.estep_stats_noalloc
+    with pytest.raises(E.AmicaError) as ei:
+        # keep = NULL means every sample counts: nkeep must then be T
+        f(1, 32, 32, 1000, 1, 3, 1, 1, 1, 1, 1, 1, 1, 0.0, 1, keep_ptr=0, nkeep=900)
+    assert ei.value.code == -3
+    with pytest.raises(E.AmicaError) as ei:
+        f(1, 64, 32, 1000, 1, 3, 1, 1, 1, 1, 1, 1, 1, 0.0, 1)     # ldx must be 32 for n = 32
+    assert ei.value.code == -3

@@ -15,7 +15,7 @@ state.
 import numpy as np
 import pytest
 
-from golden.cases import CASES, prepared, digest
+from golden.cases import CASES, prepared, digest, ref_ltall_source
 from oracle import oracle as O
 
 
@@ -114,6 +114,35 @@ def test_one_step_from_reference_state(k, prep_cache):
     for key in ("A", "alpha", "beta", "rho"):
         assert rel(getattr(orc, key), ref["iter_" + key][b]) < 1e-8, key
     assert rel(orc.mu, ref["iter_mu"][b]) < 1e-6
+
+
+@pytest.mark.parametrize("name", ["c0", "m2", "m3"])
+def test_final_lt_matches_reference_ltall(name, prep_cache):
+    """The reference's ltallfile (its Lt_h(t) of the last iteration,
+    src/amica.cu:1203-1209) against the oracle's Lt at the state entering the
+    last iteration, through the byte-offset placement of that file
+    (ref_ltall_source).  After maxiter - 1 steps of a chaotic map the two FP64
+    trajectories differ by ~1e-4 nats per channel and sample, so that is the
+    band.  With several models the Lt of a model that carries
+    almost no weight at a sample is the most sensitive quantity of the fit, so
+    m2/m3 get a wider band (measured: c0 6e-4 max / 1.1e-4 median; m2 4.6e-2 /
+    1.3e-3; m3 1.2e-2 / 6.9e-4, against a spread of Lt/n of 0.14, 5.1, 2.5)."""
+    case, ref, p = CASES[name], load(name), prep_cache[name]
+    band_max, band_med = (2e-3, 3e-4) if case.M == 1 else (0.1, 3e-3)
+    orc = make_oracle(case, p, ref, keep_Lt=True)
+    for _ in range(case.maxiter - 1):
+        orc.step()
+    orc.prepare()
+    s = orc.estep()
+    assert abs(s[0] / (case.n * case.T) - ref["ll"][-1]) < 3e-4
+    golden = ref["ltall_stride"]
+    pos, src = ref_ltall_source(case.T, 5000, 97, golden.shape[1])
+    assert len(pos) > 60
+    d = np.abs(orc.Lt[:, src] - golden[:, pos]) / case.n
+    assert d.max() < band_max, d.max()
+    assert np.median(d) < band_med, np.median(d)
+    # positions the reference never wrote hold no Lt value (its own bug)
+    assert np.all(golden[:, pos] < -1.0)
 
 
 def test_psi_against_scipy():
