@@ -20,8 +20,9 @@ oracle and against the reference's own numbers:
 
 Bands (nats per sample and channel for the LL; relative to the largest entry
 for the statistics): plain FP32 LL 2e-6, statistics 2e-5; mixed (TF32
-contractions) LL 1e-5, statistics 2e-4; the mu denominator 0.1 / 0.25 (its
-terms grow as |y| -> 0; see tests/test_engine_gpu.py).
+contractions) LL 1e-5, statistics 2e-4.  Quantities that follow the last bits
+of the data (the mu sums, per-sample Lt) are compared with the oracle run on the
+data as each form stores it; see the tests' docstrings.
 """
 import ast
 import os
@@ -34,11 +35,16 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-TIGHT = ("vs", "cn", "s2", "us", "kn", "ln", "mn", "bd", "rn", "phi")
-BANDS = {0: dict(ll=2e-6, tight=2e-5, md=0.1), 1: dict(ll=1e-5, tight=2e-4, md=0.25)}
+TIGHT = ("vs", "cn", "s2", "us", "kn", "ln", "bd", "rn", "phi")
+BANDS = {0: dict(ll=2e-6, tight=2e-5, mn=2e-5, md=0.5, md_med=1e-4),
+         1: dict(ll=1e-5, tight=2e-4, mn=2e-5, md=0.5, md_med=1e-4)}
 
 
 def _errs(s_gpu, s_orc, n, M, m):
+    """Largest error per statistic, relative to the largest entry; the mu
+    numerator relative to its Cauchy-Schwarz bound sqrt(usum * kappa num)
+    (it is a signed sum that vanishes at the fixed point); the mu denominator
+    also as the median of its per-entry relative errors."""
     a = O.split_stats(s_gpu, n, M, m)
     b = O.split_stats(s_orc, n, M, m)
     vsum = float(np.max(b["vs"]))
@@ -46,7 +52,21 @@ def _errs(s_gpu, s_orc, n, M, m):
     for k in TIGHT + ("md",):
         scale = max(float(np.max(np.abs(b[k]))), vsum if k == "cn" else 0.0)
         out[k] = float(np.max(np.abs(a[k] - b[k])) / max(scale, 1e-300))
+    cs = float(np.max(np.sqrt(np.abs(b["us"] * b["kn"]))))
+    out["mn"] = float(np.max(np.abs(a["mn"] - b["mn"])) / cs)
+    out["md_med"] = float(np.median(np.abs(a["md"] - b["md"]) / np.abs(b["md"])))
     return out
+
+
+def _as_stored(xs, precision):
+    """The sphered data as the form holds it on the GPU: FP32 (plain), or FP32
+    rounded to TF32, to nearest with ties away from zero (mixed)."""
+    a = np.ascontiguousarray(xs, dtype=np.float32).copy()
+    if precision:
+        u = a.view(np.uint32)
+        u += np.uint32(0x1000)
+        u &= np.uint32(0xFFFFE000)
+    return a.astype(np.float64)
 
 
 def _headline_data(which):
@@ -70,6 +90,15 @@ def headline():
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("which", ["n64", "n128"])
 def test_estep_matches_oracle_at_headline_shapes(which, precision, headline):
+    """Against the oracle on the exact data: the LL and the well-conditioned
+    sums.  The mu sums are signed (numerator) or grow without bound as
+    |y| -> 0 when rho -> 1 (denominator), so they follow the data's last bits:
+    the oracle on the data rounded the way the form stores it (FP32, or TF32 for
+    the mixed form) reproduces the form's distance from the exact-data oracle
+    (measured on the CPU at these shapes: mu num 1.1e-3 of its largest entry and
+    mu den 0.99 for TF32 data; 5e-7 and 2.4e-2 for FP32 data).  So they are
+    checked against the oracle on the stored data, which isolates the kernel's
+    own FP32 arithmetic."""
     from cudamica_b200.engine import Amica
     d = headline[which]
     n, T, M, m = d["n"], d["T"], d["M"], d["m"]
@@ -91,12 +120,21 @@ def test_estep_matches_oracle_at_headline_shapes(which, precision, headline):
         s_gpu = eng.estep_stats()
         dll = abs(s_gpu[0] - s_orc[0]) / (n * T)
         errs = _errs(s_gpu, s_orc, n, M, m)
+        rep = O.Oracle(_as_stored(d["xs"], precision), M, m, d["A0"], d["c0"], d["ldetS"],
+                       nthreads=8)
+        for k in ("A", "c", "alpha", "mu", "beta", "rho", "gm"):
+            getattr(rep, k)[...] = getattr(orc, k)
+        rep.prepare()
+        errs_rep = _errs(s_gpu, rep.estep(), n, M, m)
         print(f"{which} precision={precision} stage={stage} dLL={dll:.3e} "
-              + " ".join(f"{k}={v:.2e}" for k, v in errs.items()))
+              + " ".join(f"{k}={v:.2e}" for k, v in errs.items())
+              + " | stored-data oracle: mn={mn:.2e} md={md:.2e} md_med={md_med:.2e}".format(**errs_rep))
         assert dll < band["ll"], dll
         for k in TIGHT:
             assert errs[k] < band["tight"], (k, errs)
-        assert errs["md"] < band["md"], errs
+        assert errs_rep["mn"] < band["mn"], errs_rep
+        assert errs_rep["md"] < band["md"], errs_rep
+        assert errs_rep["md_med"] < band["md_med"], errs_rep
     eng.close()
 
 
@@ -145,7 +183,11 @@ def small_preps():
 @pytest.mark.parametrize("name", ["c0", "m3"])
 def test_lt_matches_oracle_at_same_parameters(name, precision, small_preps):
     """Lt_h(t) of every sample and model (amica_get_loglik) against the oracle's
-    at the same parameters: the deterministic start and after 4 iterations."""
+    at the same parameters: the deterministic start and after 4 iterations.
+    Per sample, the TF32 rounding of the stored data moves Lt by ~1e-4 nats per
+    channel (the signs are random, so the mean, the LL, moves by ~1e-6), so the
+    comparison is with the oracle on the data as the form stores it (FP32 or
+    TF32); the distance from the exact-data oracle is printed beside it."""
     from cudamica_b200.engine import Amica
     case, p = CASES[name], small_preps[name]
     eng = Amica(case.n, case.T, case.M, case.m, precision=precision,
@@ -155,6 +197,8 @@ def test_lt_matches_oracle_at_same_parameters(name, precision, small_preps):
     orc = O.Oracle(p["xs"], case.M, case.m, p["A0"], p["c0"], p["ldetS"], nthreads=8,
                    keep_Lt=True, newt_start_iter=case.newt_start_iter,
                    update_rho=int(case.update_rho))
+    rep = O.Oracle(_as_stored(p["xs"], precision), case.M, case.m, p["A0"], p["c0"],
+                   p["ldetS"], nthreads=8, keep_Lt=True)
     band = BANDS[precision]["ll"] * 4
     for stage in range(2):
         if stage == 1:
@@ -164,12 +208,18 @@ def test_lt_matches_oracle_at_same_parameters(name, precision, small_preps):
                            beta=orc.beta, rho=orc.rho)
         orc.prepare()
         orc.estep()
+        for k in ("A", "c", "alpha", "mu", "beta", "rho", "gm"):
+            getattr(rep, k)[...] = getattr(orc, k)
+        rep.prepare()
+        rep.estep()
         eng.estep_stats()
         Lt, P, _ = eng.loglik()
-        d = np.abs(Lt - orc.Lt) / case.n
-        dp = np.abs(P - orc.P) / case.n
+        d = np.abs(Lt - rep.Lt) / case.n
+        dp = np.abs(P - rep.P) / case.n
+        d_exact = np.abs(Lt - orc.Lt) / case.n
         print(f"{name} precision={precision} stage={stage} Lt max {d.max():.2e} "
-              f"median {np.median(d):.2e} P max {dp.max():.2e}")
+              f"median {np.median(d):.2e} P max {dp.max():.2e} | exact-data oracle: "
+              f"max {d_exact.max():.2e} median {np.median(d_exact):.2e}")
         # per sample (not averaged over samples): a few times the LL band
         assert d.max() < band, d.max()
         assert dp.max() < band, dp.max()

@@ -68,7 +68,10 @@ def test_noalloc_matches_context_entry_point_and_oracle(name):
     ref = eng.estep_stats()
     prm = eng.params()
     eng.close()
-    orc = O.Oracle(xs, M, m, A0, c0, ldetS, nthreads=8)
+    # the oracle on the data as this form stores it (FP32): the mu denominator
+    # follows the data's last bits near y = 0 (see test_parity_headline_gpu.py)
+    orc = O.Oracle(np.asarray(xs, dtype=np.float32).astype(np.float64), M, m, A0, c0, ldetS,
+                   nthreads=8)
     orc.prepare()
     s_orc = orc.estep()
 
@@ -100,7 +103,10 @@ def test_noalloc_matches_context_entry_point_and_oracle(name):
         print(name, "vs oracle", {k: f"{v:.1e}" for k, v in errs_o.items()})
         for k in KEYS:
             assert errs_o[k] < 2e-5, (k, errs_o)
-        assert errs_o["md"] < 0.1, errs_o
+        assert errs_o["md"] < 0.5, errs_o
+        b = O.split_stats(s_orc, n, M, m)
+        md_med = float(np.median(np.abs(O.split_stats(got, n, M, m)["md"] - b["md"]) / np.abs(b["md"])))
+        assert md_med < 1e-4, md_med
     assert np.array_equal(outs[0], outs[1])
 
 
