@@ -22,7 +22,7 @@
 
 namespace amica {
 cudaError_t launch_estep_plain(const EStepArgs& a, int NP, int nclusters, cudaStream_t st);
-cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStream_t st);
+cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStream_t st, int split);
 }
 
 using namespace amica;
@@ -101,7 +101,8 @@ cudaError_t launch_adjoint(const EStepArgs& a0, int NP, double* grad_partial, in
     a.grad_mode = 1;
     a.update_rho = 1;
     a.partial = grad_partial;
-    return use_tc ? launch_estep_tc(a, NP, nclusters, st) : launch_estep_plain(a, NP, nclusters, st);
+    a.split_phi = nullptr;   // the gradient sweep does not need phi's split correction
+    return use_tc ? launch_estep_tc(a, NP, nclusters, st, 0) : launch_estep_plain(a, NP, nclusters, st);
 }
 
 cudaError_t launch_adjoint_finalize(const double* grad_partial, double* raw, int nclusters, int n,

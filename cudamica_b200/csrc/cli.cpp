@@ -19,10 +19,12 @@
 //
 // Extension keys (not in the reference) are read afterwards by exact first
 // word, without the quirks: precision (mixed | fp32), do_reject (on/off),
-// rejsig, rejstart, rejint, maxrej, ainitfile / cinitfile (raw float32, one
-// n x n column-major block / n values per model, the last block repeated for
-// the remaining models), lrate, lratemax, lnatrate, lratefact, rho0, rholrate,
-// rhomin, rhomax, maxdec, seed.
+// rejsig, rejstart, rejint, maxrej, phi_split (split correction of phi in the
+// mixed form: 0 never, 1 always, 2 automatic) and phi_split_rel (its
+// threshold), ainitfile / cinitfile (raw float32, one n x n column-major block
+// / n values per model, the last block repeated for the remaining models),
+// lrate, lratemax, lnatrate, lratefact, rho0, rholrate, rhomin, rhomax,
+// maxdec, seed.
 //
 // Output: the reference's raw FP64 files (amica_write_outputs) and its stdout
 // lines "Iteration %lu: lrate %.16f LL %.16f ", "Likelihood decreasing!" and
@@ -268,14 +270,14 @@ int main(int argc, char** argv) {
     }
     struct { const char* k; int64_t* p; } ints[] = {{"rejstart", &cfg.rejstart}, {"rejint", &cfg.rejint},
                                                    {"maxrej", &cfg.maxrej}, {"maxdec", &cfg.maxdec},
-                                                   {"seed", &cfg.seed}};
+                                                   {"seed", &cfg.seed}, {"phi_split", &cfg.phi_split}};
     for (auto& e : ints)
         if (ext_value(L, e.k, &v)) *e.p = atol(v.c_str());
     struct { const char* k; double* p; } reals[] = {{"rejsig", &cfg.rejsig}, {"lrate", &cfg.lrate0},
                                                    {"lratemax", &cfg.lratemax}, {"lnatrate", &cfg.lnatrate},
                                                    {"lratefact", &cfg.lratefact}, {"rho0", &cfg.rho0},
                                                    {"rholrate", &cfg.rholrate}, {"rhomin", &cfg.rhomin},
-                                                   {"rhomax", &cfg.rhomax}};
+                                                   {"rhomax", &cfg.rhomax}, {"phi_split_rel", &cfg.phi_split_rel}};
     for (auto& e : reals)
         if (ext_value(L, e.k, &v)) *e.p = atof(v.c_str());
     std::string ainit, cinit;

@@ -34,12 +34,18 @@ struct Ctrl {
     int64_t iter, numdec, nkeep, nrej_total, rej_passes;
     int64_t newton, ll_decreased, no_newt, last_rejected;
     double rej_mean, rej_std;
+    // split correction of phi (tensor-core form): the largest relative change
+    // ||A_new - A|| / ||A|| of this iteration's A update (bits of a
+    // non-negative double, so that an integer max orders them), the M-step
+    // CTAs that have reported it, and the flag the E-step reads
+    uint64_t newton_rel_bits;
+    int64_t reparm_done, phi_split;
 };
 
 // One history record per iteration (read back by the host after a run).
 struct IterRec {
     double ll, lrate;
-    int64_t iter, newton, ll_decreased, nkeep, nrejected, pad;
+    int64_t iter, newton, ll_decreased, nkeep, nrejected, phi_split;
 };
 
 // Layout of one partial-sum slot (doubles), model h:
@@ -108,6 +114,9 @@ struct EStepArgs {
     const float* bext;
     float* gout;
     int ldb;
+    // tensor-core form: device flag, nonzero = form phi from hi + lo parts of
+    // both operands (split correction); nullptr = off
+    const int64_t* split_phi;
 };
 
 // The cohort E-step (one persistent launch over many single-model fits): a
@@ -145,7 +154,12 @@ struct MStepCfgHost {
     double lratemax, lnatrate, lratefact, rholrate, rhomin, rhomax, rejsig, ldetS;
     int psi_is_phi;   // 1: the E-step's n x n slot already holds phi = sum g b^T (tensor-core form)
     int psi_step;     // only every psi_step-th partial slot carries the n x n block
+    int phi_split;    // split correction of phi: 0 never, 1 always, 2 once a Newton step's relative change < phi_split_rel
+    double phi_split_rel;
 };
+// Default relative change of A below which the split correction of phi
+// switches on (phi_split = 2).
+constexpr double kPhiSplitRel = 1e-4;
 
 }  // namespace amica
 

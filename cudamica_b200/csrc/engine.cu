@@ -50,7 +50,7 @@ int tc_cohort_ctas();
 cudaError_t launch_estep_tc_cohort(const TcCohortSub* subs, const void* maps, const TcCohortItem* items,
                                    const int* item_off, int nctas, int m, cudaStream_t st);
 int tc_selftest(int mode, int N, int K, const float* hA, const float* hB, float* hD, int* derr);
-cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStream_t st);
+cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStream_t st, int split);
 // preprocess.cu
 cudaError_t launch_preprocess(const float* raw, int64_t T, int n, int do_sphere, double* means,
                               double* cov, double* sphere, double* evwork, double* ldetS_dev,
@@ -198,6 +198,7 @@ EStepArgs estep_args(amica_ctx* c) {
     a.P_out = c->d_P;
     a.partial = c->b.partial;
     a.err = c->b.err;
+    a.split_phi = c->use_tc ? &c->b.ctrl->phi_split : nullptr;
     a.T = c->T;
     a.ldx = c->NP;
     a.n = c->n;
@@ -255,7 +256,7 @@ int enqueue_estep(amica_ctx* c) {
     CK(launch_prep(c->b, c->hc, c->st));
     EStepArgs a = estep_args(c);
     if (c->use_split) TRY(enqueue_split_estep(c, a));
-    else if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st));
+    else if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st, c->hc.phi_split));
     else CK(launch_estep_plain(a, c->NP, c->nclusters, c->st));
     CK(launch_reduce_finalize(c->b, c->hc, c->nslots, c->st));
     return AMICA_OK;
@@ -302,6 +303,7 @@ void fill_out(const IterRec& r, const Ctrl& c, double ms, amica_iter_out* out) {
     out->nkeep = c.nkeep;
     out->nrejected = r.nrejected;
     out->device_ms = ms;
+    out->phi_split = r.phi_split;
 }
 
 void print_iter(const amica_ctx* c, const IterRec& r) {
@@ -340,6 +342,8 @@ int amica_default_cfg(amica_cfg* c) {
     c->device = 0;
     c->seed = 1234;
     c->verbose = 0;
+    c->phi_split = 2;
+    c->phi_split_rel = kPhiSplitRel;
     c->lrate0 = 0.1;
     c->lratemax = 1.0;
     c->lnatrate = 0.1;
@@ -429,6 +433,8 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     h.rejsig = cfg->rejsig; h.ldetS = 0.0;
     h.psi_is_phi = c->use_tc ? 1 : 0;
     h.psi_step = c->use_tc ? tc_psi_step() : 1;
+    h.phi_split = c->use_tc ? (int)cfg->phi_split : 0;
+    h.phi_split_rel = cfg->phi_split_rel;
 
     MStepBuffers& b = c->b;
     const size_t nn = (size_t)n * n, mn = (size_t)m * n;
@@ -630,6 +636,7 @@ int amica_init(amica_ctx* c, const double* A0, const double* c0) {
     ctl.lratemax = c->cfg.lratemax;
     ctl.iter = 0;
     ctl.nkeep = c->T;
+    ctl.phi_split = c->hc.phi_split == 1 ? 1 : 0;   // 2: off until the M-step switches it on
     *c->h_ctrl = ctl;
     CK(cudaMemcpyAsync(c->b.ctrl, c->h_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, c->st));
     CK(cudaMemsetAsync(c->d_keep, 1, c->T, c->st));
@@ -1004,12 +1011,12 @@ int amica_time_estep(amica_ctx* c, int64_t reps, double* ms_per_launch, int64_t*
     // one untimed launch, then reps timed back-to-back launches of the fused kernel
     // (the split form: its whole E-step, GEMMs included)
     if (c->use_split) TRY(enqueue_split_estep(c, a));
-    else if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st));
+    else if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st, c->hc.phi_split));
     else CK(launch_estep_plain(a, c->NP, c->nclusters, c->st));
     CK(cudaEventRecord(c->ev0, c->st));
     for (int64_t r = 0; r < reps; r++) {
         if (c->use_split) TRY(enqueue_split_estep(c, a));
-        else if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st));
+        else if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st, c->hc.phi_split));
         else CK(launch_estep_plain(a, c->NP, c->nclusters, c->st));
     }
     CK(cudaEventRecord(c->ev1, c->st));

@@ -68,33 +68,46 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
 }
+// try_wait with a suspend-time hint: a waiting thread sleeps until the phase
+// completes or the hint (ns) runs out, instead of spinning on issue slots the
+// density warps need.
+constexpr uint32_t kSuspendNs = 20000;
 __device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok) : "r"(addr), "r"(parity) : "memory");
+        : "=r"(ok) : "r"(addr), "r"(parity), "n"(kSuspendNs) : "memory");
     return ok != 0;
 }
 __device__ __forceinline__ bool mbar_try_cluster(uint32_t addr, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok) : "r"(addr), "r"(parity) : "memory");
+        : "=r"(ok) : "r"(addr), "r"(parity), "n"(kSuspendNs) : "memory");
     return ok != 0;
+}
+// the CTA's abort flag, read and written as shared memory
+__device__ __forceinline__ int abort_get(volatile int* f) {
+    int v;
+    asm volatile("ld.volatile.shared.u32 %0, [%1];" : "=r"(v) : "r"(smem_u32((const void*)f)) : "memory");
+    return v;
 }
 // bounded wait: false on timeout or when another thread already aborted
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
                                           int* err, bool cluster_scope = false,
                                           bool honor_abort = true) {
     const uint32_t addr = smem_u32(bar);
+    // the common case, a phase that completes within the first suspension, costs
+    // no clock read
+    if (cluster_scope ? mbar_try_cluster(addr, parity) : mbar_try(addr, parity)) return true;
     long long t0 = clock64();
     while (true) {
         if (cluster_scope ? mbar_try_cluster(addr, parity) : mbar_try(addr, parity)) return true;
-        if (honor_abort && *abort_flag) return false;
+        if (honor_abort && abort_get(abort_flag)) return false;
         if (clock64() - t0 > kWaitCycles) {
             *abort_flag = 1;
             atomicOr(err, kErrWaitTimeout);
@@ -209,6 +222,21 @@ __device__ __forceinline__ void tmem_ld4_nowait(uint32_t taddr, uint32_t* r) {
 __device__ __forceinline__ void tmem_wait_ld(uint32_t* r) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]) :: "memory");
 }
+// The same wait for several loads: one wait instruction, then an empty
+// statement per destination that keeps its uses after the wait (volatile
+// statements keep their order) without emitting anything.
+__device__ __forceinline__ void tmem_wait_ld_all() {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_after_wait(uint32_t* r) {
+    asm volatile("" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]));
+}
+// Four columns from two sample pairs (a.x, a.y, b.x, b.y).
+__device__ __forceinline__ void tmem_st4f2_nowait(uint32_t taddr, float2 a, float2 b) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};"
+                 ::"r"(taddr), "r"(__float_as_uint(a.x)), "r"(__float_as_uint(a.y)),
+                   "r"(__float_as_uint(b.x)), "r"(__float_as_uint(b.y)) : "memory");
+}
 // Tensor-memory column of chunk c (kSub columns) of the log2|y| cache: the
 // 16-column gaps after the two b buffers when a chunk fits there, then the 128
 // columns after W_lo.
@@ -249,16 +277,19 @@ __device__ __forceinline__ uint32_t sw128_off(int row, int col, int rows) {
     return (uint32_t)(blk * rows * 128 + row * 128 + ((((c >> 2) ^ (row & 7)) & 7) << 4) + ((c & 3) << 2));
 }
 
-template <int NP>
+// SPLIT: the form with the split correction of phi (one x stage; the G and b
+// tiles twice as wide, their low parts in columns [kS, 2 kS)).
+template <int NP, bool SPLIT = false>
 struct TcShape {
     static constexpr int KB = NP / 32;                       // 128-B column blocks of x / W
+    static constexpr int NSTAGE = SPLIT ? 1 : 2;             // x stages
+    static constexpr int TCOLS = SPLIT ? 2 * kS : kS;        // columns of the G / b tiles
     static constexpr uint32_t W_BYTES = 128u * NP * 4u;      // 128 rows x NP
     static constexpr uint32_t X_BYTES = (uint32_t)kS * NP * 4u;
-    static constexpr uint32_t G_BYTES = 128u * 128u * 2u;    // 128 rows x 2 blocks of 32 samples
+    static constexpr uint32_t G_BYTES = 128u * 128u * ((TCOLS + 31) / 32);   // 128 rows x 32-column blocks
     static constexpr uint32_t OFF_W = 0;
     static constexpr uint32_t OFF_X0 = OFF_W + W_BYTES;
-    static constexpr uint32_t OFF_X1 = OFF_X0 + X_BYTES;
-    static constexpr uint32_t OFF_G = OFF_X1 + X_BYTES;
+    static constexpr uint32_t OFF_G = OFF_X0 + NSTAGE * X_BYTES;
     static constexpr uint32_t OFF_BT = OFF_G + G_BYTES;                  // b tile, same layout as G
     // per-warp channel sums of Lt from every model's CTA: [2][8 models][4 warps][kS] f32
     static constexpr uint32_t OFF_SLOT = OFF_BT + G_BYTES;
@@ -269,6 +300,7 @@ struct TcShape {
     static constexpr uint32_t BYTES = OFF_MISC + 64;
     static constexpr uint32_t TMEM_COLS = 512;   // b: [0,48) [64,112); phi: [128,128+NP); W_lo: [256,256+NP);
                                                  // log2|y| cache: [48,64) [112,128) [384,512)
+    static_assert(BYTES + 1024 <= 232448, "shared memory");
 };
 
 enum { BAR_FULL0 = 0, BAR_FULL1, BAR_EMPTY0, BAR_EMPTY1, BAR_BFULL0, BAR_BFULL1, BAR_BEMPTY0,
@@ -288,16 +320,19 @@ struct TcArgs {
     int ngroups;   // partial slots per cluster: kWG per sample set, set-major
 };
 
-template <int NP, int MM, int R>
+template <int NP, int MM, int R, bool SPLIT>
 __global__ void __launch_bounds__(kThreads, 1)
     estep_tc_kernel(const __grid_constant__ CUtensorMap xmap, TcArgs ta) {
-    using Sh = TcShape<NP>;
+    using Sh = TcShape<NP, SPLIT>;
     const EStepArgs& a = ta.e;
+    // Both forms are launched when the split correction can switch on during a
+    // fit (the switch is a device-side flag, so that the iteration's graph does
+    // not change); the one that does not match the flag leaves at once.
+    if ((a.split_phi != nullptr && *a.split_phi != 0) != SPLIT) return;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // 1024-byte alignment for the swizzled operand tiles
     uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     float* Wsm = (float*)(sm + Sh::OFF_W);
-    float* Gsm = (float*)(sm + Sh::OFF_G);
     float* slot = (float*)(sm + Sh::OFF_SLOT);
     uint64_t* bar = (uint64_t*)(sm + Sh::OFF_BAR);
     uint32_t* tmem_holder = (uint32_t*)(sm + Sh::OFF_MISC);
@@ -443,8 +478,8 @@ __device__ __forceinline__ void tc_cohort_density(uint8_t* sm, uint64_t* bar, vo
                                                   const EStepArgs& a, const TcCohortItem& itm,
                                                   uint32_t tmem, int warp, int lane) {
     constexpr int NP = 128;
+    constexpr bool SPLIT = false;
     using Sh = TcShape<NP>;
-    float* Gsm = (float*)(sm + Sh::OFF_G);
     float* slot = (float*)(sm + Sh::OFF_SLOT);
     const int h = 0, M = a.M, n = a.n;
     const int ntile_local = itm.ntiles;
@@ -459,6 +494,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     estep_tc_cohort_kernel(const TcCohortSub* __restrict__ subs, const CUtensorMap* __restrict__ maps,
                            const TcCohortItem* __restrict__ items, const int* __restrict__ item_off) {
     constexpr int NP = 128;
+    constexpr bool SPLIT = false;
     using Sh = TcShape<NP>;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -671,9 +707,9 @@ int tc_pack(int n) { return 128 / tc_np(n); }
 
 // a.x holds at least ceil(T / R) * R samples of a.ldx = npc floats (samples at
 // and beyond T zero); it is read as ceil(T / R) rows of 128 floats.
-template <int NP, int MM, int R>
+template <int NP, int MM, int R, bool SPLIT>
 cudaError_t launch_tc(const EStepArgs& a, int nclusters, cudaStream_t st) {
-    using Sh = TcShape<NP>;
+    using Sh = TcShape<NP, SPLIT>;
     PFN_encodeTiled enc = get_encode();
     if (!enc) return cudaErrorNotSupported;
     if (a.ldx * R != NP) return cudaErrorInvalidValue;
@@ -689,7 +725,7 @@ cudaError_t launch_tc(const EStepArgs& a, int nclusters, cudaStream_t st) {
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
     const size_t smem = Sh::BYTES + 1024;
-    auto kern = estep_tc_kernel<NP, MM, R>;
+    auto kern = estep_tc_kernel<NP, MM, R, SPLIT>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     TcArgs ta;
@@ -714,7 +750,7 @@ template <int NP, int MM, int R>
 int tc_active_clusters(int M) {
     using Sh = TcShape<NP>;
     const size_t smem = Sh::BYTES + 1024;
-    auto kern = estep_tc_kernel<NP, MM, R>;
+    auto kern = estep_tc_kernel<NP, MM, R, false>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return -1;
     cudaLaunchConfig_t cfg = {};
@@ -849,16 +885,28 @@ cudaError_t launch_estep_tc_cohort(const TcCohortSub* subs, const void* maps, co
     }
 }
 
-cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStream_t st) {
-    if (NP != tc_np(a.n) || a.ldx != NP) return cudaErrorInvalidValue;
+// split: 0 the plain instantiation only, 1 the split-correction one only, 2
+// both (each leaves at once unless the device flag a.split_phi selects it).
+template <bool SPLIT>
+cudaError_t launch_tc_form(const EStepArgs& a, int nclusters, cudaStream_t st) {
     const int R = tc_pack(a.n);
 #define AMICA_TC_CASE(MMV) \
-    if (a.m == MMV) return R == 1 ? launch_tc<128, MMV, 1>(a, nclusters, st) \
-                                  : (R == 2 ? launch_tc<128, MMV, 2>(a, nclusters, st) \
-                                            : launch_tc<128, MMV, 4>(a, nclusters, st));
+    if (a.m == MMV) return R == 1 ? launch_tc<128, MMV, 1, SPLIT>(a, nclusters, st) \
+                                  : (R == 2 ? launch_tc<128, MMV, 2, SPLIT>(a, nclusters, st) \
+                                            : launch_tc<128, MMV, 4, SPLIT>(a, nclusters, st));
     AMICA_TC_CASE(1) AMICA_TC_CASE(2) AMICA_TC_CASE(3) AMICA_TC_CASE(4) AMICA_TC_CASE(5)
 #undef AMICA_TC_CASE
     return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStream_t st, int split) {
+    if (NP != tc_np(a.n) || a.ldx != NP) return cudaErrorInvalidValue;
+    if (split != 1) {
+        const cudaError_t e = launch_tc_form<false>(a, nclusters, st);
+        if (e != cudaSuccess) return e;
+    }
+    if (split != 0) return launch_tc_form<true>(a, nclusters, st);
+    return cudaSuccess;
 }
 
 }  // namespace amica

@@ -751,20 +751,62 @@ __global__ void __launch_bounds__(256) k_gemm64(GemmArgs g) {
 // Reparametrisation and c update after the A update (src/amica.cu:2367-2512):
 // unit columns of A, mu *= norm, beta /= norm^2, mu -= W_old (cnew - c), c = cnew.
 // One CTA of 1024 threads per model (n <= 256).
+// With phi_split = 2, every CTA also reports ||A_new - A||_F / ||A||_F of its
+// model (frozen models report nothing), and the last CTA to finish switches the
+// split correction of phi on for good once a Newton iteration changed no
+// model's A by more than phi_split_rel.
 __global__ void __launch_bounds__(1024) k_reparm(int update_A, int do_reparm, double* A,
                                                  const double* __restrict__ Anew,
                                                  const double* __restrict__ W, double* c,
                                                  double* mu, double* beta,
                                                  const double* __restrict__ work,
-                                                 const int* __restrict__ use_newton, int n, int m) {
+                                                 const int* __restrict__ use_newton, int n, int m,
+                                                 int phi_split, double phi_split_rel, Ctrl* ctrl) {
     const int h = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (use_newton[h] < 0) return;                    // frozen model: A, c, mu, beta unchanged
+    auto report = [&](double rel, bool frozen) {
+        if (phi_split != 2 || tid != 0) return;
+        if (!frozen) atomicMax((unsigned long long*)&ctrl->newton_rel_bits,
+                               (unsigned long long)__double_as_longlong(rel));
+        __threadfence();
+        if (atomicAdd((unsigned long long*)&ctrl->reparm_done, 1ull) == (unsigned long long)(gridDim.x - 1)) {
+            __threadfence();
+            const double mx = __longlong_as_double((long long)atomicMax(
+                (unsigned long long*)&ctrl->newton_rel_bits, 0ull));
+            if (update_A && ctrl->newton && mx < phi_split_rel) ctrl->phi_split = 1;
+        }
+    };
+    if (use_newton[h] < 0) {                          // frozen model: A, c, mu, beta unchanged
+        report(0.0, true);
+        return;
+    }
     const double* cnew = work + (size_t)h * 4 * n + 3 * n;
     double* ch = c + (size_t)h * n;
     __shared__ double norms[kMaxN], shift[kMaxN], dc[kMaxN];
+    __shared__ double red[2][32];
+    double rel = 0.0;
     if (update_A) {
         double* Ah = A + (size_t)h * n * n;
         const double* An = Anew + (size_t)h * n * n;
+        if (phi_split == 2) {
+            double dd = 0.0, aa = 0.0;
+            for (int e = tid; e < n * n; e += blockDim.x) {
+                const double d = An[e] - Ah[e];
+                dd += d * d;
+                aa += Ah[e] * Ah[e];
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                dd += __shfl_xor_sync(0xffffffffu, dd, o);
+                aa += __shfl_xor_sync(0xffffffffu, aa, o);
+            }
+            if (lane == 0) { red[0][warp] = dd; red[1][warp] = aa; }
+            __syncthreads();
+            if (tid == 0) {
+                double sd = 0.0, sa = 0.0;
+                for (int w = 0; w < (int)(blockDim.x >> 5); w++) { sd += red[0][w]; sa += red[1][w]; }
+                rel = sa > 0.0 ? sqrt(sd / sa) : 0.0;
+            }
+            __syncthreads();
+        }
         if (do_reparm) {
             for (int cc = warp; cc < n; cc += 32) {
                 double s = 0.0;
@@ -802,6 +844,7 @@ __global__ void __launch_bounds__(1024) k_reparm(int update_A, int do_reparm, do
         __syncthreads();
     }
     for (int i = tid; i < n; i += blockDim.x) ch[i] = cnew[i];   // src/amica.cu:2456-2462
+    report(rel, false);
 }
 
 // ---------------------------------------------------------------------------
@@ -875,6 +918,7 @@ struct MCfg {
     int do_newton, update_rho, rho_start_iter, newt_start_iter, maxdec;
     int update_gm, update_alpha, update_A, update_mu, update_beta, do_reparm;
     int do_reject, rejstart, rejint, maxrej;
+    int phi_split;
     double lratemax, lnatrate, lratefact, rholrate, rhomin, rhomax, rejsig;
 };
 
@@ -1013,6 +1057,10 @@ __global__ void k_ctrl(MCfg cf, const double* __restrict__ stats, Ctrl* ctrl,
     }
     c.iter = iter;
     c.last_rejected = 0;
+    // the A update of this iteration reports its relative change (k_reparm)
+    c.newton_rel_bits = 0;
+    c.reparm_done = 0;
+    if (cf.phi_split != 2) c.phi_split = cf.phi_split;
     *ctrl = c;
     if (hist && iter - 1 < hist_cap) {
         IterRec r;
@@ -1023,7 +1071,7 @@ __global__ void k_ctrl(MCfg cf, const double* __restrict__ stats, Ctrl* ctrl,
         r.ll_decreased = c.ll_decreased;
         r.nkeep = c.nkeep;
         r.nrejected = 0;
-        r.pad = 0;
+        r.phi_split = c.phi_split;          // the form this iteration's E-step ran
         hist[iter - 1] = r;
     }
 }
@@ -1120,7 +1168,7 @@ static MCfg to_mcfg(const MStepCfgHost& h) {
     c.newt_start_iter = h.newt_start_iter; c.maxdec = h.maxdec; c.update_gm = h.update_gm;
     c.update_alpha = h.update_alpha; c.update_A = h.update_A; c.update_mu = h.update_mu;
     c.update_beta = h.update_beta; c.do_reparm = h.do_reparm; c.do_reject = h.do_reject;
-    c.rejstart = h.rejstart; c.rejint = h.rejint; c.maxrej = h.maxrej;
+    c.rejstart = h.rejstart; c.rejint = h.rejint; c.maxrej = h.maxrej; c.phi_split = h.phi_split;
     c.lratemax = h.lratemax; c.lnatrate = h.lnatrate; c.lratefact = h.lratefact;
     c.rholrate = h.rholrate; c.rhomin = h.rhomin; c.rhomax = h.rhomax; c.rejsig = h.rejsig;
     return c;
@@ -1209,7 +1257,7 @@ cudaError_t launch_mstep(const MStepBuffers& b, const MStepCfgHost& h, const flo
         k_gemm64<<<g, 256, 0, st>>>(ga);
     }
     k_reparm<<<h.M, 1024, 0, st>>>(h.update_A, h.do_reparm, b.A, b.Anew, b.W, b.c, b.mu, b.beta,
-                                  b.work, b.use_newton, h.n, h.m);
+                                  b.work, b.use_newton, h.n, h.m, h.phi_split, h.phi_split_rel, b.ctrl);
     {
         const int64_t nA = (int64_t)h.M * h.n * h.n, nmix = (int64_t)h.M * h.m * h.n;
         const int grid = (int)std::min<int64_t>((nA + 255) / 256, 148);

@@ -30,9 +30,9 @@ CFG_INT_FIELDS = (
     "nchannels", "nsamples", "nmmodels", "nsdm", "maxiter", "do_sphere", "block_size", "fix_init",
     "do_newton", "update_rho", "rho_start_iter", "newt_start_iter", "maxdec", "update_gm",
     "update_alpha", "update_A", "update_mu", "update_beta", "do_reparm", "do_reject", "rejstart",
-    "rejint", "maxrej", "precision", "device", "seed", "verbose", "max_clusters")
+    "rejint", "maxrej", "precision", "device", "seed", "verbose", "max_clusters", "phi_split")
 CFG_DBL_FIELDS = ("lrate0", "lratemax", "lnatrate", "lratefact", "rho0", "rholrate", "rhomin",
-                  "rhomax", "rejsig")
+                  "rhomax", "rejsig", "phi_split_rel")
 
 EXPORTED = (
     "amica_default_cfg", "amica_create", "amica_destroy", "amica_load_data",
@@ -52,7 +52,8 @@ class Cfg(C.Structure):
 
 class IterOut(C.Structure):
     _fields_ = [("iter", _i64), ("ll", _dbl), ("lrate", _dbl), ("ll_decreased", _i64),
-                ("newton", _i64), ("nkeep", _i64), ("nrejected", _i64), ("device_ms", _dbl)]
+                ("newton", _i64), ("nkeep", _i64), ("nrejected", _i64), ("device_ms", _dbl),
+                ("phi_split", _i64)]
 
 
 class Paths(C.Structure):

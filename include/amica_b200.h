@@ -61,7 +61,12 @@ typedef struct amica_cfg {
     int64_t precision, device, seed, verbose;
     int64_t max_clusters;   /* cap on the E-step grid in clusters (0: as many as fit); lets
                                several contexts share the GPU's SMs concurrently (new key) */
+    int64_t phi_split;      /* mixed form: form phi = sum g b^T from hi + lo TF32 parts of
+                               both operands: 0 never, 1 always, 2 (default) from the
+                               iteration after a Newton step changed every model's A by
+                               less than phi_split_rel (relative, Frobenius) (new key) */
     double lrate0, lratemax, lnatrate, lratefact, rho0, rholrate, rhomin, rhomax, rejsig;
+    double phi_split_rel;   /* the threshold of phi_split = 2 (default 1e-4) (new key) */
 } amica_cfg;
 
 /* What one iteration reports; the reference prints the same quantities
@@ -75,6 +80,8 @@ typedef struct amica_iter_out {
     int64_t nkeep;         /* samples in the sums (T minus rejected) */
     int64_t nrejected;     /* samples dropped by this iteration's rejection pass */
     double  device_ms;     /* device time of the iteration (CUDA events) */
+    int64_t phi_split;     /* 1 if this iteration's E-step formed phi with the split
+                              (hi + lo) correction (mixed form) */
 } amica_iter_out;
 
 typedef struct amica_ctx amica_ctx;

@@ -293,6 +293,29 @@ int amo_preprocess(const float *x, int64_t n, int64_t T, int64_t do_sphere,
 
 /* ---------------------------------------------------------------- E-step */
 
+/* Per-sample arithmetic type.  The default build is FP64 throughout; built
+ * with -DAMO_FP32_ESTEP (liboracle32.so) the per-sample quantities (b, y, the
+ * densities, z, Lt, P, v, g) are FP32 and only the sums over samples stay
+ * FP64: the FP32 host rendering that the CPU baseline times beside the FP64
+ * one.  The M-step is FP64 in both. */
+#ifdef AMO_FP32_ESTEP
+typedef float ereal;
+#define EPOW powf
+#define EEXP expf
+#define ELOG logf
+#define EFABS fabsf
+#define ECOPYSIGN copysignf
+#define ETINY ((float)TINY_ABS)
+#else
+typedef double ereal;
+#define EPOW pow
+#define EEXP exp
+#define ELOG log
+#define EFABS fabs
+#define ECOPYSIGN copysign
+#define ETINY TINY_ABS
+#endif
+
 typedef struct {
     const amo_cfg *cfg;
     amo_state *st;
@@ -308,58 +331,75 @@ static void *estep_worker(void *arg) {
     amo_state *st = w->st;
     const int64_t n = cfg->n, M = cfg->M, m = cfg->m, T = cfg->T;
     const amo_off o = offsets(n, m);
-    double *b = malloc(sizeof(double) * M * n);
-    double *y = malloc(sizeof(double) * M * m * n);
-    double *z = malloc(sizeof(double) * M * m * n);
-    double *Lt = malloc(sizeof(double) * M);
-    double *v = malloc(sizeof(double) * M);
-    double *g = malloc(sizeof(double) * n);
+    ereal *b = malloc(sizeof(ereal) * M * n);
+    ereal *y = malloc(sizeof(ereal) * M * m * n);
+    ereal *z = malloc(sizeof(ereal) * M * m * n);
+    ereal *Lt = malloc(sizeof(ereal) * M);
+    ereal *v = malloc(sizeof(ereal) * M);
+    ereal *g = malloc(sizeof(ereal) * n);
+    ereal *xt = malloc(sizeof(ereal) * n);
+    /* the parameters in the per-sample type */
+    ereal *W = malloc(sizeof(ereal) * M * n * n);
+    ereal *wc = malloc(sizeof(ereal) * M * n);
+    ereal *sqb = malloc(sizeof(ereal) * M * m * n);
+    ereal *mu = malloc(sizeof(ereal) * M * m * n);
+    ereal *rho = malloc(sizeof(ereal) * M * m * n);
+    ereal *Cq = malloc(sizeof(ereal) * M * m * n);
+    for (int64_t e = 0; e < M * n * n; e++) W[e] = (ereal)st->W[e];
+    for (int64_t e = 0; e < M * n; e++) wc[e] = (ereal)w->wc[e];
+    for (int64_t e = 0; e < M * m * n; e++) {
+        sqb[e] = (ereal)w->sqb[e];
+        mu[e] = (ereal)st->mu[e];
+        rho[e] = (ereal)st->rho[e];
+        Cq[e] = (ereal)w->Cq[e];
+    }
     double *acc = w->acc;
 
     for (int64_t t = w->t0; t < w->t1; t++) {
-        const double *xt = w->x + t * n;
+        const double *xd = w->x + t * n;
+        for (int64_t k = 0; k < n; k++) xt[k] = (ereal)xd[k];
         for (int64_t h = 0; h < M; h++) {
             /* b = W x - W c: cublasDgemm + Dgemv + substract, src/amica.cu:1054-1102 */
-            const double *Wh = st->W + h * n * n;
-            double *bh = b + h * n;
-            for (int64_t i = 0; i < n; i++) bh[i] = 0.0;
+            const ereal *Wh = W + h * n * n;
+            ereal *bh = b + h * n;
+            for (int64_t i = 0; i < n; i++) bh[i] = 0;
             for (int64_t k = 0; k < n; k++) {
-                double xk = xt[k];
-                const double *col = Wh + k * n;
+                ereal xk = xt[k];
+                const ereal *col = Wh + k * n;
                 for (int64_t i = 0; i < n; i++) bh[i] += col[i] * xk;
             }
-            for (int64_t i = 0; i < n; i++) bh[i] -= w->wc[h * n + i];
-            double sum_lse = 0.0;
+            for (int64_t i = 0; i < n; i++) bh[i] -= wc[h * n + i];
+            ereal sum_lse = 0;
             for (int64_t i = 0; i < n; i++) {
-                double q[64];
-                double qmax = -INFINITY;
+                ereal q[64];
+                ereal qmax = -INFINITY;
                 for (int64_t j = 0; j < m; j++) {
                     int64_t idx = (h * m + j) * n + i;
                     /* betabyxminusmu, src/kernels.cu:251-272 */
-                    double yv = w->sqb[idx] * (bh[i] - st->mu[idx]);
+                    ereal yv = sqb[idx] * (bh[i] - mu[idx]);
                     y[idx] = yv;
-                    double ay = fabs(yv);
-                    if (ay < TINY_ABS) ay = TINY_ABS;
+                    ereal ay = EFABS(yv);
+                    if (ay < ETINY) ay = ETINY;
                     /* logalogblogpfun, src/kernels.cu:282-307 */
-                    q[j] = w->Cq[idx] - pow(ay, st->rho[idx]);
+                    q[j] = Cq[idx] - EPOW(ay, rho[idx]);
                     if (q[j] > qmax) qmax = q[j];
                 }
                 /* updateltz, src/kernels.cu:317-366 */
-                double s = 0.0;
-                for (int64_t j = 0; j < m; j++) s += exp(q[j] - qmax);
-                double lse = qmax + log(s);
-                for (int64_t j = 0; j < m; j++) z[(h * m + j) * n + i] = 1.0 / exp(lse - q[j]);
+                ereal s = 0;
+                for (int64_t j = 0; j < m; j++) s += EEXP(q[j] - qmax);
+                ereal lse = qmax + ELOG(s);
+                for (int64_t j = 0; j < m; j++) z[(h * m + j) * n + i] = (ereal)1 / EEXP(lse - q[j]);
                 sum_lse += lse;
             }
-            Lt[h] = w->ltc[h] + sum_lse;
+            Lt[h] = (ereal)w->ltc[h] + sum_lse;
         }
         /* updatell, src/kernels.cu:376-450 */
-        double lmax = Lt[0];
+        ereal lmax = Lt[0];
         for (int64_t h = 1; h < M; h++) if (Lt[h] > lmax) lmax = Lt[h];
-        double s = 0.0;
-        for (int64_t h = 0; h < M; h++) s += exp(Lt[h] - lmax);
-        double P = lmax + log(s);
-        for (int64_t h = 0; h < M; h++) v[h] = 1.0 / exp(P - Lt[h]);
+        ereal s = 0;
+        for (int64_t h = 0; h < M; h++) s += EEXP(Lt[h] - lmax);
+        ereal P = lmax + ELOG(s);
+        for (int64_t h = 0; h < M; h++) v[h] = (ereal)1 / EEXP(P - Lt[h]);
         if (st->Lt) for (int64_t h = 0; h < M; h++) st->Lt[h * T + t] = Lt[h];
         if (st->P) st->P[t] = P;
         if (st->keep && !st->keep[t]) continue;
@@ -367,63 +407,64 @@ static void *estep_worker(void *arg) {
         acc[0] += P;
         for (int64_t h = 0; h < M; h++) {
             double *A = acc + 1 + h * o.S;
-            const double vh = v[h];
-            const double *bh = b + h * n;
+            const ereal vh = v[h];
+            const ereal *bh = b + h * n;
             A[o.vs] += vh;                                   /* Dasum, src/amica.cu:1585 */
             for (int64_t i = 0; i < n; i++) {
                 A[o.cn + i] += vh * xt[i];                   /* cnew Dgemv, :1280-1292 */
                 A[o.s2 + i] += vh * (bh[i] * bh[i]);         /* pow2 + Dgemv, :1300-1323 */
-                g[i] = 0.0;
+                g[i] = 0;
             }
             for (int64_t j = 0; j < m; j++) {
                 for (int64_t i = 0; i < n; i++) {
                     int64_t idx = (h * m + j) * n + i;
-                    double rho = st->rho[idx];
-                    double u = vh * z[idx];                  /* computeu, src/kernels.cu:473-484 */
-                    double yv = y[idx];
-                    double ay = fabs(yv);
-                    if (ay < TINY_ABS) ay = TINY_ABS;
+                    ereal rh = rho[idx];
+                    ereal u = vh * z[idx];                   /* computeu, src/kernels.cu:473-484 */
+                    ereal yv = y[idx];
+                    ereal ay = EFABS(yv);
+                    if (ay < ETINY) ay = ETINY;
                     /* computefp, src/kernels.cu:540-553 */
-                    double fp = rho * copysign(pow(ay, rho - 1.0), yv);
-                    double ufp = u * fp;
-                    g[i] += w->sqb[idx] * ufp;               /* computeg, :561-574 */
+                    ereal fp = rh * ECOPYSIGN(EPOW(ay, rh - 1), yv);
+                    ereal ufp = u * fp;
+                    g[i] += sqb[idx] * ufp;                  /* computeg, :561-574 */
                     int64_t mi = j * n + i;
                     A[o.us + mi] += u;                       /* getusum, :495-532 */
                     A[o.kn + mi] += ufp * fp;                /* getdkappanumer, :583-621 */
-                    double yy = yv;
+                    ereal yy = yv;
                     if (cfg->ref_y_slab_bug) {               /* OFFSET4D2D(y, j, h, M) */
                         int64_t slab = h * M + j;
                         yy = y[slab * n + i];
                     }
-                    double ayy = fabs(yy);
-                    if (ayy < TINY_ABS) ayy = TINY_ABS;
-                    double yys = copysign(ayy, yy);
-                    double lv = fp * yy - 1.0;               /* getdlambdanumer, :630-671 */
+                    ereal ayy = EFABS(yy);
+                    if (ayy < ETINY) ayy = ETINY;
+                    ereal yys = ECOPYSIGN(ayy, yy);
+                    ereal lv = fp * yy - 1;                  /* getdlambdanumer, :630-671 */
                     A[o.ln + mi] += u * (lv * lv);
                     A[o.mn + mi] += ufp;                     /* getbetamu, :680-763 */
-                    if (rho <= 2.0) {
+                    if (rh <= 2) {
                         A[o.md + mi] += ufp / yys;
                         A[o.bd + mi] += ufp * yy;
                     } else {
                         A[o.md + mi] += ufp * fp;
-                        A[o.bd + mi] += u * pow(ayy, rho);
+                        A[o.bd + mi] += u * EPOW(ayy, rh);
                     }
                     if (cfg->update_rho) {                   /* getdrhonumer, :785-827 */
-                        double pv = pow(ayy, rho);
-                        A[o.rn + mi] += u * (pv * log(pv));
+                        ereal pv = EPOW(ayy, rh);
+                        A[o.rn + mi] += u * (pv * ELOG(pv));
                     }
                 }
             }
             /* phi = g b^T, src/amica.cu:1535-1550 */
             double *phi = A + o.phi;
             for (int64_t k = 0; k < n; k++) {
-                double bk = bh[k];
+                ereal bk = bh[k];
                 double *col = phi + k * n;
                 for (int64_t i = 0; i < n; i++) col[i] += g[i] * bk;
             }
         }
     }
-    free(b); free(y); free(z); free(Lt); free(v); free(g);
+    free(b); free(y); free(z); free(Lt); free(v); free(g); free(xt);
+    free(W); free(wc); free(sqb); free(mu); free(rho); free(Cq);
     return NULL;
 }
 

@@ -15,6 +15,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
+LIB32_PATH = os.path.join(HERE, "liboracle32.so")
 
 _i64 = C.c_int64
 _dbl = C.c_double
@@ -43,15 +44,17 @@ def build() -> None:
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-_lib = None
+_libs = {}
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
+def lib(fp32: bool = False):
+    """liboracle.so, or with fp32=True liboracle32.so: the same iteration with
+    its E-step's per-sample arithmetic in FP32 (sums over samples in FP64)."""
+    if fp32 not in _libs:
+        path = LIB32_PATH if fp32 else LIB_PATH
+        if not os.path.exists(path):
             build()
-        L = C.CDLL(LIB_PATH)
+        L = C.CDLL(path)
         L.amo_stats_len.restype = _i64
         L.amo_stats_len.argtypes = [_i64, _i64, _i64]
         L.amo_default_cfg.argtypes = [C.POINTER(Cfg)]
@@ -66,8 +69,8 @@ def lib():
         L.amo_jacobi_eig.argtypes = [_pd, _i64, _pd, _pd]
         L.amo_psi.restype = _dbl
         L.amo_psi.argtypes = [_dbl]
-        _lib = L
-    return _lib
+        _libs[fp32] = L
+    return _libs[fp32]
 
 
 def _p(a):
@@ -142,11 +145,11 @@ class Oracle:
 
     def __init__(self, xs: np.ndarray, M: int, m: int, A0: np.ndarray, c0: np.ndarray,
                  ldetS: float, nthreads: int = 8, keep_P: bool = True, keep_Lt: bool = False,
-                 **cfg_over):
+                 fp32: bool = False, **cfg_over):
         self.x = np.ascontiguousarray(xs, dtype=np.float64)
         T, n = self.x.shape
         self.n, self.T, self.M, self.m = n, T, M, m
-        L = lib()
+        self._L = L = lib(fp32)
         self.cfg = Cfg()
         L.amo_default_cfg(C.byref(self.cfg))
         self.cfg.n, self.cfg.T, self.cfg.M, self.cfg.m = n, T, M, m
@@ -181,20 +184,20 @@ class Oracle:
 
     def step(self) -> float:
         self.lrate_hist.append(self.st.lrate)
-        rc = lib().amo_em_step(C.byref(self.cfg), C.byref(self.st), _p(self.x), _p(self.stats))
+        rc = self._L.amo_em_step(C.byref(self.cfg), C.byref(self.st), _p(self.x), _p(self.stats))
         if rc != 0:
             raise RuntimeError(f"oracle step failed: {rc}")
         self.ll_hist.append(self.st.ll)
         return self.st.ll
 
     def prepare(self) -> None:
-        rc = lib().amo_prepare(C.byref(self.cfg), C.byref(self.st))
+        rc = self._L.amo_prepare(C.byref(self.cfg), C.byref(self.st))
         if rc != 0:
             raise RuntimeError(f"oracle prepare failed: {rc}")
 
     def estep(self) -> np.ndarray:
         """Sufficient statistics at the current parameters (after prepare())."""
-        rc = lib().amo_estep(C.byref(self.cfg), C.byref(self.st), _p(self.x), _p(self.stats))
+        rc = self._L.amo_estep(C.byref(self.cfg), C.byref(self.st), _p(self.x), _p(self.stats))
         if rc != 0:
             raise RuntimeError(f"oracle estep failed: {rc}")
         return self.stats.copy()
