@@ -1,4 +1,5 @@
-"""Benchmark: EM iterations/s of the AMICA engine on one B200 (or N replicas).
+"""Benchmark: EM iterations/s of the AMICA engine on one B200, or of one fit
+sharded over N B200s.
 
 Workload (the metric's configuration): n=128 channels, T=1,000,000 samples,
 M=3 models, m=3 mixtures, synthetic FP32 data from cudamica_b200.synth
@@ -13,6 +14,10 @@ form's iterations/s with the data resident in HBM, timed with CUDA events on
 the engine's stream, max over ranks; the plain FP32 form is timed the same way
 and reported beside it, with both forms' final LL after a fixed-length fit.
 `e2e` runs a whole fit through the public C ABI from pinned host memory.
+Under torchrun with N > 1 ranks the samples are split over the ranks (one
+fit, strong scaling: each iteration is the shards' E-steps, one NCCL
+all-reduce of the sufficient statistics, the same M-step on every rank);
+`--replicas` runs N independent fits instead.
 `--impl reference` times the reference's own implementation (its CUDA sources
 compiled here for sm_100a, oracle/_ref/cudaamica_ref) on the same workload,
 using its own per-iteration timer.
@@ -154,6 +159,46 @@ def traffic_per_launch():
         return None
     m = re.search(r"traffic_bytes_per_launch_n128_T1e6:\s*(\d+)", open(p).read())
     return int(m.group(1)) if m else None
+
+
+def roofline_for(estep_ms: float, T: int, clocks: dict, kernel: str) -> dict:
+    """The binding (largest) of the algorithmic bounds of one E-step launch over
+    T samples at the workload's n, M, m, against its CUDA-event time."""
+    hbm, bf16, src = peaks()
+    n, M, m = (WORKLOAD[k] for k in ("n", "M", "m"))
+    est = estep_ms * 1e-3
+    alg_bytes = 4 * n * T + 4 * M * T            # x read once + Lt write per iteration
+    tc_flops = 4 * M * n * n * T                 # W x and g b^T
+    mufu = (4 * m + 1) * M * n * T               # lg2, ex2, ex2, rcp per element + lg2 per (h, i, t)
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    mufu_peak = 16 * 148 * sm_mhz * 1e6          # ops/s
+    tf32_peak = 0.5 * bf16 * 1e12                # flop/s
+    bounds = {
+        "hbm": {"time_s": alg_bytes / (hbm * 1e9), "achieved": alg_bytes / est / 1e9, "peak": hbm,
+                "unit": "GB/s", "per_launch": alg_bytes},
+        "tensor": {"time_s": tc_flops / tf32_peak, "achieved": tc_flops / est / 1e12,
+                   "peak": tf32_peak / 1e12, "unit": "TFLOP/s", "per_launch": tc_flops},
+        "sfu": {"time_s": mufu / mufu_peak, "achieved": mufu / est / 1e9, "peak": mufu_peak / 1e9,
+                "unit": "Gop/s", "per_launch": mufu},
+    }
+    for v in bounds.values():
+        v["frac"] = v["time_s"] / est
+    bind = max(bounds, key=lambda k: bounds[k]["time_s"])
+    b = bounds[bind]
+    tr = traffic_per_launch()
+    return {"bound": bind, "achieved": b["achieved"], "peak": b["peak"], "unit": b["unit"],
+            "frac": b["frac"],
+            "traffic": None if tr is None else int(tr * T / WORKLOAD["T"]),
+            "kernel": kernel, "kernel_ms": estep_ms, "samples_per_launch": T,
+            "all_bounds": bounds,
+            "peaks_used": {
+                "hbm": f"{hbm} GB/s, {src} copy bandwidth (MEASURED_PEAKS.json)",
+                "tensor": f"TF32 = half of the {src} BF16 burst rate {bf16} TFLOP/s "
+                          "(dense TF32 is half of dense BF16 on B200; TF32 not measured)",
+                "sfu": f"16 MUFU ops/clk/SM x 148 SMs x {sm_mhz:.0f} MHz (sampled SM clock)"},
+            "note": "the binding (largest) of the algorithmic bounds of one E-step launch, "
+                    "divided by its CUDA-event time; FP32 non-tensor work is not among the "
+                    "algorithmic counts"}
 
 
 def time_form(x, A0, c0, precision, device, steps, warmup, fit_iters):
@@ -455,6 +500,97 @@ def profile_case(args):
     return 0
 
 
+def sharded_arm(args, ws: int, rank: int, local: int):
+    """One fit of the workload with its samples split over the ranks (strong
+    scaling): each rank loads its contiguous sample range, the sphering is
+    formed from the column sums and scatters of all ranks, and every EM
+    iteration is the shard's E-step, one NCCL all-reduce of the statistics
+    vector and the same M-step on every rank (cudamica_b200.sharded).  A step
+    is one iteration of the whole T-sample fit."""
+    import torch
+    import torch.distributed as dist
+    from cudamica_b200.engine import Amica
+    from cudamica_b200.sharded import EngineShard, ShardedFit, engine_shard_preprocess, shard_range
+    n, T, M, m = (WORKLOAD[k] for k in ("n", "T", "M", "m"))
+    dev = torch.device("cuda", local)
+    x, A0, c0 = make_data()
+    t0, t1 = shard_range(T, rank, ws)
+    xs = np.ascontiguousarray(x[t0:t1])
+    del x
+
+    def fit_setup(data):
+        eng = Amica(n, t1 - t0, M, m, precision=1, device=local, maxiter=4000)
+        eng.load_data(data)
+        engine_shard_preprocess(eng, T, group=dist.group.WORLD)
+        eng.init(A0, c0)
+        return eng, ShardedFit(EngineShard(eng), T, group=dist.group.WORLD, device=dev)
+
+    eng, fit = fit_setup(xs)
+    for _ in range(args.warmup):
+        fit.step()
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        e0.record(st)
+        outs = fit.run(args.steps)
+        e1.record(st)
+        torch.cuda.synchronize()
+    clocks = clk.summary()
+    ms_rank = e0.elapsed_time(e1) / args.steps
+    est_ms, _ = eng.time_estep(5)
+    # the exchange alone: the statistics all-reduce, 20 times
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    a0.record(st)
+    for _ in range(20):
+        dist.all_reduce(fit.buf, op=dist.ReduceOp.SUM)
+    a1.record(st)
+    torch.cuda.synchronize()
+    ar_ms = a0.elapsed_time(a1) / 20
+    kernel, lpi = eng.kernel, eng.launches_per_iteration
+    eng.close()
+    ms, est_max, ar_max = reduce_over_ranks([ms_rank, est_ms, ar_ms], dist, "max")
+    e2e = None
+    if not args.no_e2e:
+        pin = pinned_copy(xs)
+        dist.barrier()
+        w0 = time.perf_counter()
+        eng2, fit2 = fit_setup(pin.numpy())
+        fit2.run(args.steps)
+        prm = eng2.params()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - w0
+        eng2.close()
+        del pin
+        wall = reduce_over_ranks([wall], dist, "max")[0]
+        e2e = {"value": args.steps / wall, "unit": "iters/s",
+               "h2d_bytes_per_step": xs.nbytes * ws / args.steps,
+               "d2h_bytes_per_step": (sum(v.nbytes for v in prm.values()) + args.steps * 64) * ws / args.steps,
+               "scope": f"per rank: load_data of its shard from pinned memory, sharded sphering, init, "
+                        f"{args.steps} sharded iterations, get_params; wall clock, max over ranks"}
+    out = {
+        "metric": METRIC, "value": 1000.0 / ms, "unit": "iters/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "n=128 T=1e6 M=3 m=3, one EM iteration of the whole fit per step", **WORKLOAD,
+                   "precision": "mixed: tcgen05 TF32 contractions, FP32 densities, FP64 M-step",
+                   "kernel": kernel, "parallelism": f"samples sharded over {ws} GPUs, "
+                                                    "one FP64 all-reduce of the statistics per iteration",
+                   "samples_per_rank": t1 - t0,
+                   "l2": "inputs larger than L2 (512 MB sphered data in all, per step)"},
+        "allreduce_ms": ar_max, "stats_bytes": int(fit.buf.numel() * 8),
+        "final_ll": outs[-1].ll,
+        "roofline": roofline_for(est_max, t1 - t0, clocks, kernel),
+        "gpu_launches": lpi * args.steps,
+        "clocks": clocks,
+    }
+    if e2e is not None:
+        out["e2e"] = e2e
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -464,6 +600,8 @@ def main():
     ap.add_argument("--fit-iters", type=int, default=1000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with N > 1 GPUs: N independent fits instead of one sample-sharded fit")
     ap.add_argument("--profile-case", action="store_true",
                     help="no timing: run a few fused E-step launches of both forms on a "
                          "T-sample slice (for ncu captures)")
@@ -527,6 +665,14 @@ def main():
         print(json.dumps(line))
         return 0
 
+    if ws > 1 and not args.replicas:
+        out = sharded_arm(args, ws, rank, local)
+        if rank == 0:
+            print(json.dumps(out))
+        pg.barrier()
+        pg.destroy_process_group()
+        return 0
+
     import torch
     device = local
     torch.cuda.set_device(device)
@@ -554,40 +700,7 @@ def main():
         same[fit] = {"mixed": lm, "plain": lp, "abs_diff": abs(lm - lp)}
     ms, t_plain = reduce_over_ranks([rm["ms"], rp["ms"]], pg, "max")
     value = whole_job_rate(ms, ws)
-    hbm, bf16, src = peaks()
-    n, T, M, m = (WORKLOAD[k] for k in ("n", "T", "M", "m"))
-    est = rm["estep_ms"] * 1e-3
-    alg_bytes = 4 * n * T + 4 * M * T            # x read once + Lt write per iteration
-    tc_flops = 4 * M * n * n * T                 # W x and g b^T
-    mufu = (4 * m + 1) * M * n * T               # lg2, ex2, ex2, rcp per element + lg2 per (h, i, t)
-    sm_mhz = clocks.get("sm_mhz") or 1965.0
-    mufu_peak = 16 * 148 * sm_mhz * 1e6          # ops/s
-    tf32_peak = 0.5 * bf16 * 1e12                # flop/s
-    bounds = {
-        "hbm": {"time_s": alg_bytes / (hbm * 1e9), "achieved": alg_bytes / est / 1e9, "peak": hbm,
-                "unit": "GB/s", "per_launch": alg_bytes},
-        "tensor": {"time_s": tc_flops / tf32_peak, "achieved": tc_flops / est / 1e12,
-                   "peak": tf32_peak / 1e12, "unit": "TFLOP/s", "per_launch": tc_flops},
-        "sfu": {"time_s": mufu / mufu_peak, "achieved": mufu / est / 1e9, "peak": mufu_peak / 1e9,
-                "unit": "Gop/s", "per_launch": mufu},
-    }
-    for v in bounds.values():
-        v["frac"] = v["time_s"] / est
-    bind = max(bounds, key=lambda k: bounds[k]["time_s"])
-    b = bounds[bind]
-    roof = {"bound": bind, "achieved": b["achieved"], "peak": b["peak"], "unit": b["unit"],
-            "frac": b["frac"],
-            "traffic": traffic_per_launch(),
-            "kernel": rm["kernel"], "kernel_ms": rm["estep_ms"],
-            "all_bounds": bounds,
-            "peaks_used": {
-                "hbm": f"{hbm} GB/s, {src} copy bandwidth (MEASURED_PEAKS.json)",
-                "tensor": f"TF32 = half of the {src} BF16 burst rate {bf16} TFLOP/s "
-                          "(dense TF32 is half of dense BF16 on B200; TF32 not measured)",
-                "sfu": f"16 MUFU ops/clk/SM x 148 SMs x {sm_mhz:.0f} MHz (sampled SM clock)"},
-            "note": "the binding (largest) of the algorithmic bounds of one E-step launch, "
-                    "divided by its CUDA-event time; FP32 non-tensor work is not among the "
-                    "algorithmic counts"}
+    roof = roofline_for(rm["estep_ms"], WORKLOAD["T"], clocks, rm["kernel"])
     out = {
         "metric": METRIC, "value": value, "unit": "iters/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -595,7 +708,7 @@ def main():
         "config": {"workload": "n=128 T=1e6 M=3 m=3, one EM iteration per step", **WORKLOAD,
                    "precision": "mixed: tcgen05 TF32 contractions, FP32 densities, FP64 M-step",
                    "kernel": rm["kernel"], "l2": "inputs larger than L2 (512 MB sphered data per step)",
-                   "parallelism": "replicas" if ws > 1 else "single GPU",
+                   "parallelism": "independent replicas" if ws > 1 else "single GPU",
                    "estep_clusters": rm["grid"]},
         "plain_fp32": {"value": whole_job_rate(t_plain, ws), "ms_per_step": t_plain,
                        "kernel": rp["kernel"], "estep_ms": rp["estep_ms"], "estep_clusters": rp["grid"]},

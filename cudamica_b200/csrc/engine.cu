@@ -54,9 +54,17 @@ cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStrea
 // preprocess.cu
 cudaError_t launch_preprocess(const float* raw, int64_t T, int n, int do_sphere, double* means,
                               double* cov, double* sphere, double* evwork, double* ldetS_dev,
-                              float* x, int ldx, int tf32, int* err, cudaStream_t st);
+                              float* x, int ldx, int tf32, int* err, cudaStream_t st,
+                              long long fault_wait_cycles);
 cudaError_t launch_convert_sphered(const double* xs, int64_t T, int n, float* x, int ldx, int tf32,
                                    cudaStream_t st);
+cudaError_t launch_shard_colsum(const float* raw, int64_t T, int n, double* sums, cudaStream_t st);
+cudaError_t launch_shard_scatter(const float* raw, int64_t T, int n, const double* sums, int64_t T_total,
+                                 double* means, double* scatter, cudaStream_t st);
+cudaError_t launch_shard_finish(const float* raw, int64_t T, int n, int do_sphere, const double* means,
+                                const double* scatter, int64_t T_total, double* cov, double* sphere,
+                                double* evwork, double* ldetS_dev, float* x, int ldx, int tf32, int* err,
+                                cudaStream_t st);
 // adjoint.cu
 cudaError_t launch_adjoint(const EStepArgs& a, int NP, double* grad_partial, int nclusters,
                            cudaStream_t st, bool use_tc);
@@ -95,6 +103,7 @@ struct amica_ctx {
     int nclusters = 0, ntiles = 0, nslots = 0;   // nslots: partial-sum slots per model
     int nclusters_cap = 0;                        // grid the partial-sum buffer was sized for
     bool have_data = false, have_x = false, have_init = false, have_estep = false;
+    bool have_shard_mean = false;   // amica_shard_scatter has set the mean of all shards
 
     float* d_rawx = nullptr;     // T x n raw input (float)
     float* d_x = nullptr;        // T x NP sphered (float)
@@ -113,6 +122,7 @@ struct amica_ctx {
     double* d_grad = nullptr;
 
     Ctrl* h_ctrl = nullptr;       // pinned
+    long long fault_wait_cycles = 0;   // amica_test_arm_wait_fault: armed for the next preprocess
     int* h_err = nullptr;         // pinned
     std::vector<IterRec> hist;    // host copy of the iteration history
 
@@ -550,9 +560,11 @@ int amica_preprocess(amica_ctx* c) {
     if (!c) return AMICA_ERR_INVALIDPARAM;
     if (!c->have_data) return AMICA_ERR_STATE;
     CK(cudaSetDevice(c->dev));
+    const long long fault = c->fault_wait_cycles;
+    c->fault_wait_cycles = 0;                      // the hook arms one launch
     CK(launch_preprocess(c->d_rawx, c->T, c->n, (int)c->cfg.do_sphere, c->d_means, c->d_cov,
                          c->d_sphere, c->d_evwork, c->d_ldetS, c->d_x, c->NP, (c->use_tc || c->use_split) ? 1 : 0,
-                         c->b.err, c->st));
+                         c->b.err, c->st, fault));
     double ld = 0.0;
     CK(cudaMemcpyAsync(&ld, c->d_ldetS, sizeof(double), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -865,6 +877,11 @@ int amica_loglik_adjoint(amica_ctx* c, double* ll, double* dW, double* dmu, doub
         ncl = c->adj_nclusters;
         nsl = ncl * plain_partial_groups(n);
         a.nclusters = ncl;
+        // its channel blocks each write only their own channels of a slot, and
+        // the split form's E-step leaves whole slots of another layout in this
+        // buffer: start from zero
+        PartLayout PL{n, m};
+        CK(cudaMemsetAsync(c->b.partial, 0, sizeof(double) * (size_t)nsl * M * PL.stride(), c->st));
     }
     CK(launch_adjoint(a, c->NP, c->b.partial, ncl, c->st, c->use_tc));
     CK(launch_adjoint_finalize(c->b.partial, c->b.raw, nsl, n, m, M, c->b.A, c->b.c,
@@ -977,6 +994,105 @@ int amica_write_outputs(amica_ctx* c, const amica_paths* p) {
 }
 
 int amica_last_cuda_error(void) { return g_last_cuda_error; }
+
+// ---- sample-sharded fits: the E-step of one shard, then the M-step from the
+// statistics of all shards (added by the caller, e.g. one all-reduce)
+__global__ void k_set_nkeep(Ctrl* ctrl, int64_t nkeep) { ctrl->nkeep = nkeep; }
+
+int amica_shard_estep(amica_ctx* c, double* d_stats) {
+    if (!c || !d_stats) return AMICA_ERR_INVALIDPARAM;
+    if (!c->have_x || !c->have_init) return AMICA_ERR_STATE;
+    if (c->hc.do_reject) return AMICA_ERR_UNSUPPORTED;   // the rejection rule needs every sample's P
+    CK(cudaSetDevice(c->dev));
+    TRY(snapshot_params(c, false));
+    CK(cudaEventRecord(c->ev0, c->st));
+    TRY(enqueue_estep(c));
+    CK(cudaMemcpyAsync(d_stats, c->b.stats, sizeof(double) * amica_stats_len(c->n, c->M, c->m),
+                       cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->have_estep = true;
+    return check_device_error(c);
+}
+
+int amica_shard_mstep(amica_ctx* c, const double* d_stats, int64_t nkeep_total, amica_iter_out* out) {
+    if (!c || !d_stats || nkeep_total < 1) return AMICA_ERR_INVALIDPARAM;
+    if (!c->have_estep) return AMICA_ERR_STATE;
+    CK(cudaSetDevice(c->dev));
+    CK(cudaMemcpyAsync(c->b.stats, d_stats, sizeof(double) * amica_stats_len(c->n, c->M, c->m),
+                       cudaMemcpyDeviceToDevice, c->st));
+    // the M-step normalises by the samples of every shard (LL, gm); the next
+    // E-step of this shard counts its own again
+    k_set_nkeep<<<1, 1, 0, c->st>>>(c->b.ctrl, nkeep_total);
+    CK(launch_mstep(c->b, c->hc, c->d_P, c->d_keep, c->T, c->st));
+    k_set_nkeep<<<1, 1, 0, c->st>>>(c->b.ctrl, c->T);
+    CK(cudaEventRecord(c->ev1, c->st));
+    CK(cudaMemcpyAsync(c->h_ctrl, c->b.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    int e = check_device_error(c);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    const Ctrl ctl = *c->h_ctrl;
+    if (e == AMICA_OK && !std::isfinite(ctl.ll)) e = AMICA_ERR_NUMERIC;
+    if (e != AMICA_OK) {
+        snapshot_params(c, true);
+        cudaStreamSynchronize(c->st);
+        return e;
+    }
+    IterRec r{};
+    CK(cudaMemcpy(&r, c->b.hist + (ctl.iter - 1), sizeof(IterRec), cudaMemcpyDeviceToHost));
+    r.nkeep = nkeep_total;
+    c->hist.push_back(r);
+    print_iter(c, r);
+    fill_out(r, ctl, ms, out);
+    if (out) out->nkeep = nkeep_total;
+    return AMICA_OK;
+}
+
+int amica_shard_colsum(amica_ctx* c, double* d_sums) {
+    if (!c || !d_sums) return AMICA_ERR_INVALIDPARAM;
+    if (!c->have_data) return AMICA_ERR_STATE;
+    CK(cudaSetDevice(c->dev));
+    CK(launch_shard_colsum(c->d_rawx, c->T, c->n, d_sums, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return check_device_error(c);
+}
+
+int amica_shard_scatter(amica_ctx* c, const double* d_sums_total, int64_t T_total, double* d_scatter) {
+    if (!c || !d_sums_total || !d_scatter || T_total < c->T) return AMICA_ERR_INVALIDPARAM;
+    if (!c->have_data) return AMICA_ERR_STATE;
+    CK(cudaSetDevice(c->dev));
+    CK(launch_shard_scatter(c->d_rawx, c->T, c->n, d_sums_total, T_total, c->d_means, d_scatter, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    TRY(check_device_error(c));
+    c->have_shard_mean = true;
+    return AMICA_OK;
+}
+
+int amica_shard_sphere(amica_ctx* c, const double* d_scatter_total, int64_t T_total) {
+    if (!c || !d_scatter_total || T_total < c->T || T_total < 2) return AMICA_ERR_INVALIDPARAM;
+    if (!c->have_data || !c->have_shard_mean) return AMICA_ERR_STATE;
+    CK(cudaSetDevice(c->dev));
+    CK(launch_shard_finish(c->d_rawx, c->T, c->n, (int)c->cfg.do_sphere, c->d_means, d_scatter_total, T_total,
+                           c->d_cov, c->d_sphere, c->d_evwork, c->d_ldetS, c->d_x, c->NP,
+                           (c->use_tc || c->use_split) ? 1 : 0, c->b.err, c->st));
+    double ld = 0.0;
+    CK(cudaMemcpyAsync(&ld, c->d_ldetS, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    TRY(check_device_error(c));
+    c->ldetS = ld;
+    c->hc.ldetS = ld;
+    c->have_x = true;
+    c->have_shard_mean = false;
+    return AMICA_OK;
+}
+
+int amica_test_arm_wait_fault(amica_ctx* c, int64_t wait_cycles) {
+    if (!c || wait_cycles <= 0) return AMICA_ERR_INVALIDPARAM;
+    // the cooperative eigensolver (and its grid barriers) runs above 128 channels
+    if (c->n <= 128 || c->cfg.do_sphere != 1) return AMICA_ERR_UNSUPPORTED;
+    c->fault_wait_cycles = (long long)wait_cycles;
+    return AMICA_OK;
+}
 
 int64_t amica_launches_per_iteration(amica_ctx* c) { return c ? launches_per_iteration(c) : 0; }
 

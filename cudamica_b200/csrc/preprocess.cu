@@ -31,22 +31,34 @@ __global__ void k_colsum(const float* __restrict__ x, int64_t T, int n, double* 
     }
 }
 
-__global__ void k_mean(const double* __restrict__ part, int nblk, int n, int64_t T,
+// mean = (sum of the per-CTA partial sums) / div; div = 1 gives the sums
+__global__ void k_mean(const double* __restrict__ part, int nblk, int n, double div,
                        double* __restrict__ mean) {
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         double s = 0.0;
         for (int b = 0; b < nblk; b++) s += part[(size_t)b * n + i];
-        mean[i] = s / (double)T;
+        mean[i] = s / div;
     }
 }
 
-__global__ void k_cov_reduce(const double* __restrict__ part, int nblk, int n, int64_t T,
+__global__ void k_cov_reduce(const double* __restrict__ part, int nblk, int n, double div,
                              double* __restrict__ C) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n * n) return;
     double s = 0.0;
     for (int b = 0; b < nblk; b++) s += part[(size_t)b * n * n + e];
-    C[e] = s / (double)T;
+    C[e] = s / div;
+}
+
+// The sharded form's inputs to k_sphere: the covariance (scatter / T) and, for
+// do_sphere 2, the per-channel variance (scatter diagonal / (T - 1)) of all
+// shards.
+__global__ void k_scale_scatter(const double* __restrict__ scatter, int n, double T,
+                                double* __restrict__ C, double* __restrict__ var) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n * n; e += blockDim.x * gridDim.x) {
+        C[e] = scatter[e] / T;
+        if (e % (n + 1) == 0) var[e / (n + 1)] = scatter[e] / (T - 1.0);
+    }
 }
 
 // S = V diag(2/sqrt(d)) V^T (do_sphere 1), diag(1/std) (2) or I (0); ldetS.
@@ -367,17 +379,19 @@ __global__ void __launch_bounds__(256, 1) k_cov8q(const float* __restrict__ x, i
 // barrier number b completes when it reaches (b + 1) * gridDim.x.  The wait is
 // bounded (~1 s); on expiry it records kErrWaitTimeout and sets *abort, after
 // which every block leaves its loops at the next barrier.
+// (skip_arrival: the test hook of amica_test_arm_wait_fault, a block that does
+// not arrive, so that the others' waits run out.)
 __device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned target, volatile int* abort,
-                                             int* err) {
+                                             int* err, long long wait_cycles, bool skip_arrival = false) {
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
-        atomicAdd(count, 1u);
+        if (!skip_arrival) atomicAdd(count, 1u);
         const long long t0 = clock64();
         while (true) {
             const unsigned v = *(volatile unsigned*)count;
             if (v >= target || *abort) break;
-            if (clock64() - t0 > 2000000000LL) {
+            if (clock64() - t0 > wait_cycles) {
                 *abort = 1;
                 atomicOr(err, amica::kErrWaitTimeout);
                 break;
@@ -401,6 +415,8 @@ struct JacGlobal {
     double* part;      // per-block partial sums of the stopping test, 2 per block
     unsigned* count;   // barrier counter (zero at launch)
     int* abort;        // zero at launch
+    long long wait_cycles;   // bound of every barrier wait (~1 s)
+    int skip_block;          // test hook: this block skips its first arrival (-1: none)
 };
 __global__ void __launch_bounds__(kJacThreads, 1) k_jacobi_grid(const double* __restrict__ C,
                                                                 double* __restrict__ V,
@@ -421,7 +437,8 @@ __global__ void __launch_bounds__(kJacThreads, 1) k_jacobi_grid(const double* __
         if (r <= c) ap[pk_idx(r, c)] = C[e];
         V[e] = (r == c) ? 1.0 : 0.0;
     }
-    if (!grid_barrier(g.count, (++bar) * gridDim.x, g.abort, err)) return;
+    if (!grid_barrier(g.count, (++bar) * gridDim.x, g.abort, err, g.wait_cycles,
+                      (int)blockIdx.x == g.skip_block)) return;
     for (int sweep = 0; sweep < 40; sweep++) {
         double off = 0.0, tot = 0.0;
         for (int e = gtid; e < np; e += gthreads) {
@@ -452,7 +469,7 @@ __global__ void __launch_bounds__(kJacThreads, 1) k_jacobi_grid(const double* __
             for (int w = 0; w < kJacThreads / 32; w++) s += red[w];
             g.part[2 * blockIdx.x + 1] = s;
         }
-        if (!grid_barrier(g.count, (++bar) * gridDim.x, g.abort, err)) return;
+        if (!grid_barrier(g.count, (++bar) * gridDim.x, g.abort, err, g.wait_cycles)) return;
         // every block sums the partials in the same order and takes the same decision
         double offt = 0.0, tott = 0.0;
         for (int b = 0; b < (int)gridDim.x; b++) {
@@ -482,7 +499,7 @@ __global__ void __launch_bounds__(kJacThreads, 1) k_jacobi_grid(const double* __
             }
             // every block has read the diagonal entries that the round's K = L
             // blocks are about to overwrite
-            if (!grid_barrier(g.count, (++bar) * gridDim.x, g.abort, err)) return;
+            if (!grid_barrier(g.count, (++bar) * gridDim.x, g.abort, err, g.wait_cycles)) return;
             // A <- J^T A J: block (K, L), K <= L, numbered column by column
             for (int e = gtid; e < nblk; e += gthreads) {
                 int L = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
@@ -525,7 +542,7 @@ __global__ void __launch_bounds__(kJacThreads, 1) k_jacobi_grid(const double* __
                 V[(size_t)p * n + r] = c * vp - s * vq;
                 V[(size_t)q * n + r] = s * vp + c * vq;
             }
-            if (!grid_barrier(g.count, (++bar) * gridDim.x, g.abort, err)) return;
+            if (!grid_barrier(g.count, (++bar) * gridDim.x, g.abort, err, g.wait_cycles)) return;
         }
     }
     for (int i = gtid; i < n; i += gthreads) evals[i] = __ldcg(ap + pk_idx(i, i));
@@ -656,50 +673,72 @@ __global__ void k_convert(const double* __restrict__ xs, int64_t T, int n, float
     }
 }
 
-}  // namespace
-
-namespace amica {
-
-// evwork: >= 4 n^2 + 4 n doubles
-cudaError_t launch_preprocess(const float* raw, int64_t T, int n, int do_sphere, double* means,
-                              double* cov, double* sphere, double* evwork, double* ldetS_dev,
-                              float* x, int ldx, int tf32, int* err, cudaStream_t st) {
-    if (n > 256 || ldx > 256) return cudaErrorInvalidValue;
-    const bool big = n > 128;
-    const int nblk = (int)((T + kChunk - 1) / kChunk);
+// The preprocessing of one fit in three steps, so that a fit whose samples are
+// spread over several contexts can add the sums of every shard between them:
+//   pp_colsum:  column sums / div of the raw data;
+//   pp_scatter: sum_t (x_t - mean)(x_t - mean)^T / div (do_sphere 1 only);
+//   pp_finish:  the eigendecomposition of the covariance, S and ldetS, and
+//               the sphered data x = S (raw - mean) in the layout of the E-step.
+// part: scratch of pp_part_len doubles; evwork: >= 4 n^2 + 4 n doubles.
+int sm_count() {
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const int ncov = nsm;
-    const int64_t chunk = ((T + ncov - 1) / ncov + kCovRows - 1) / kCovRows * kCovRows;
-    double* part = nullptr;
-    size_t part_len = (size_t)nblk * n;
-    if ((size_t)ncov * n * n > part_len) part_len = (size_t)ncov * n * n;
-    cudaError_t e = cudaMallocAsync(&part, sizeof(double) * part_len, st);
-    if (e != cudaSuccess) return e;
+    return nsm;
+}
+
+size_t pp_part_len(int64_t T, int n) {
+    const size_t nblk = (size_t)((T + kChunk - 1) / kChunk);
+    const size_t a = nblk * n, b = (size_t)sm_count() * n * n;
+    return a > b ? a : b;
+}
+
+cudaError_t pp_colsum(const float* raw, int64_t T, int n, double div, double* part, double* out,
+                      cudaStream_t st) {
+    const int nblk = (int)((T + kChunk - 1) / kChunk);
     k_colsum<<<nblk, 256, 0, st>>>(raw, T, n, part);
-    k_mean<<<1, 256, 0, st>>>(part, nblk, n, T, means);
+    k_mean<<<1, 256, 0, st>>>(part, nblk, n, div, out);
+    return cudaGetLastError();
+}
+
+cudaError_t pp_scatter(const float* raw, int64_t T, int n, const double* means, double div,
+                       double* part, double* out, cudaStream_t st) {
+    const int ncov = sm_count();
+    const int64_t chunk = ((T + ncov - 1) / ncov + kCovRows - 1) / kCovRows * kCovRows;
+    if (n <= 128) {
+        k_cov8<<<ncov, 256, 0, st>>>(raw, T, n, chunk, means, part);
+    } else {
+        const size_t csmem = sizeof(double) * 2 * kCovRows * 128;
+        cudaError_t e = cudaFuncSetAttribute(k_cov8q, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem);
+        if (e != cudaSuccess) return e;
+        k_cov8q<<<dim3(ncov, 4), 256, csmem, st>>>(raw, T, n, chunk, means, part);
+    }
+    k_cov_reduce<<<(n * n + 255) / 256, 256, 0, st>>>(part, ncov, n, div, out);
+    return cudaGetLastError();
+}
+
+// var_ready: evwork's variance slot already holds the do_sphere 2 variances
+cudaError_t pp_finish(const float* raw, int64_t T, int n, int do_sphere, const double* means,
+                      const double* cov, double* sphere, double* evwork, double* ldetS_dev,
+                      float* x, int ldx, int tf32, int* err, double* part, bool var_ready,
+                      cudaStream_t st, long long fault_wait_cycles) {
+    const bool big = n > 128;
+    const int nsm = sm_count();
+    cudaError_t e = cudaSuccess;
     double* V = evwork;
     double* ev = evwork + (size_t)n * n;
     double* var = ev + n;
     if (do_sphere == 1 && !big) {
-        k_cov8<<<ncov, 256, 0, st>>>(raw, T, n, chunk, means, part);
-        k_cov_reduce<<<(n * n + 255) / 256, 256, 0, st>>>(part, ncov, n, T, cov);
         const size_t jsmem = sizeof(double) * (size_t)((((n * (n + 1)) / 2 + 1) & ~1) + n * n);
         e = cudaFuncSetAttribute(k_jacobi_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)jsmem);
-        if (e != cudaSuccess) { cudaFreeAsync(part, st); return e; }
+        if (e != cudaSuccess) return e;
         k_jacobi_smem<<<1, kJacThreads, jsmem, st>>>(cov, V, ev, n);
     } else if (do_sphere == 1) {
-        const size_t csmem = sizeof(double) * 2 * kCovRows * 128;
-        e = cudaFuncSetAttribute(k_cov8q, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem);
-        if (e != cudaSuccess) { cudaFreeAsync(part, st); return e; }
-        k_cov8q<<<dim3(ncov, 4), 256, csmem, st>>>(raw, T, n, chunk, means, part);
-        k_cov_reduce<<<(n * n + 255) / 256, 256, 0, st>>>(part, ncov, n, T, cov);
-        // Jacobi state in the (now free) partial buffer: packed triangle, the
-        // stopping-test partials, the barrier counter and the abort flag
+        // Jacobi state in the partial buffer: packed triangle, the stopping-test
+        // partials, the barrier counter and the abort flag
         int per_sm = 0;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi_grid, kJacThreads, 0);
-        if (e != cudaSuccess || per_sm < 1) { cudaFreeAsync(part, st); return e ? e : cudaErrorInvalidValue; }
+        if (e != cudaSuccess || per_sm < 1) return e ? e : cudaErrorInvalidValue;
         const int nb = nsm < 64 ? nsm : 64;
         const size_t np = (size_t)n * (n + 1) / 2;
         JacGlobal jg;
@@ -707,33 +746,104 @@ cudaError_t launch_preprocess(const float* raw, int64_t T, int n, int do_sphere,
         jg.part = part + np;
         jg.count = reinterpret_cast<unsigned*>(part + np + 2 * nb);
         jg.abort = reinterpret_cast<int*>(part + np + 2 * nb + 1);
+        jg.wait_cycles = fault_wait_cycles > 0 ? fault_wait_cycles : 2000000000LL;
+        jg.skip_block = fault_wait_cycles > 0 ? 0 : -1;
         e = cudaMemsetAsync(part + np + 2 * nb, 0, 2 * sizeof(double), st);
-        if (e != cudaSuccess) { cudaFreeAsync(part, st); return e; }
-        void* args[] = {(void*)&cov, (void*)&V, (void*)&ev, (void*)&n, (void*)&jg, (void*)&err};
+        if (e != cudaSuccess) return e;
+        double* covp = const_cast<double*>(cov);
+        void* args[] = {(void*)&covp, (void*)&V, (void*)&ev, (void*)&n, (void*)&jg, (void*)&err};
         e = cudaLaunchCooperativeKernel((const void*)k_jacobi_grid, dim3(nb), dim3(kJacThreads), args, 0, st);
-        if (e != cudaSuccess) { cudaFreeAsync(part, st); return e; }
-    } else if (do_sphere == 2) {
+        if (e != cudaSuccess) return e;
+    } else if (do_sphere == 2 && !var_ready) {
         k_var<<<n, 256, 0, st>>>(raw, T, n, means, var);
     }
     k_sphere<<<(n * n + 255) / 256, 256, 0, st>>>(V, ev, var, n, do_sphere, sphere, ldetS_dev);
     if (big) {
         const size_t smemq = sizeof(double) * (256 * 64 + kSphTileQ * 257);
         e = cudaFuncSetAttribute(k_apply_sphere_q, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemq);
-        if (e != cudaSuccess) { cudaFreeAsync(part, st); return e; }
+        if (e != cudaSuccess) return e;
         const int64_t ntq = (T + kSphTileQ - 1) / kSphTileQ;
         const int gq = (int)(ntq < nsm ? ntq : nsm);
         k_apply_sphere_q<<<dim3(gq, (ldx + 63) / 64), 512, smemq, st>>>(raw, T, n, means, sphere, x, ldx, tf32);
-        cudaFreeAsync(part, st);
         return cudaGetLastError();
     }
     const size_t smem2 = sizeof(double) * (128 * 128 + kSphTile * 129);
     e = cudaFuncSetAttribute(k_apply_sphere8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);
-    if (e != cudaSuccess) { cudaFreeAsync(part, st); return e; }
+    if (e != cudaSuccess) return e;
     const int64_t ntile = (T + kSphTile - 1) / kSphTile;
     const int gsph = (int)(ntile < nsm ? ntile : nsm);
     k_apply_sphere8<<<gsph, 512, smem2, st>>>(raw, T, n, means, sphere, x, ldx, tf32);
-    cudaFreeAsync(part, st);
     return cudaGetLastError();
+}
+
+}  // namespace
+
+namespace amica {
+
+// fault_wait_cycles > 0 arms the test hook of amica_test_arm_wait_fault for
+// this launch (cooperative eigensolver only: block 0 skips its first arrival,
+// every wait is bounded by fault_wait_cycles).
+cudaError_t launch_preprocess(const float* raw, int64_t T, int n, int do_sphere, double* means,
+                              double* cov, double* sphere, double* evwork, double* ldetS_dev,
+                              float* x, int ldx, int tf32, int* err, cudaStream_t st,
+                              long long fault_wait_cycles) {
+    if (n > 256 || ldx > 256) return cudaErrorInvalidValue;
+    double* part = nullptr;
+    cudaError_t e = cudaMallocAsync(&part, sizeof(double) * pp_part_len(T, n), st);
+    if (e != cudaSuccess) return e;
+    e = pp_colsum(raw, T, n, (double)T, part, means, st);
+    if (e == cudaSuccess && do_sphere == 1) e = pp_scatter(raw, T, n, means, (double)T, part, cov, st);
+    if (e == cudaSuccess)
+        e = pp_finish(raw, T, n, do_sphere, means, cov, sphere, evwork, ldetS_dev, x, ldx, tf32, err, part,
+                      false, st, fault_wait_cycles);
+    cudaFreeAsync(part, st);
+    return e;
+}
+
+// Sharded preprocessing: the column sums of this shard's raw data (n doubles).
+cudaError_t launch_shard_colsum(const float* raw, int64_t T, int n, double* sums, cudaStream_t st) {
+    if (n > 256) return cudaErrorInvalidValue;
+    double* part = nullptr;
+    cudaError_t e = cudaMallocAsync(&part, sizeof(double) * pp_part_len(T, n), st);
+    if (e != cudaSuccess) return e;
+    e = pp_colsum(raw, T, n, 1.0, part, sums, st);
+    cudaFreeAsync(part, st);
+    return e;
+}
+
+// means = sums / T_total (the column sums of all shards), then the scatter of
+// this shard's raw data about them, n x n doubles.
+cudaError_t launch_shard_scatter(const float* raw, int64_t T, int n, const double* sums, int64_t T_total,
+                                 double* means, double* scatter, cudaStream_t st) {
+    if (n > 256 || T_total < 1) return cudaErrorInvalidValue;
+    double* part = nullptr;
+    cudaError_t e = cudaMallocAsync(&part, sizeof(double) * pp_part_len(T, n), st);
+    if (e != cudaSuccess) return e;
+    k_mean<<<1, 256, 0, st>>>(sums, 1, n, (double)T_total, means);
+    e = pp_scatter(raw, T, n, means, 1.0, part, scatter, st);
+    cudaFreeAsync(part, st);
+    return e;
+}
+
+// S and ldetS from the scatter of all shards (T_total samples; do_sphere 1 and
+// 2 read it, 0 ignores it), applied to this shard's samples.
+cudaError_t launch_shard_finish(const float* raw, int64_t T, int n, int do_sphere, const double* means,
+                                const double* scatter, int64_t T_total, double* cov, double* sphere,
+                                double* evwork, double* ldetS_dev, float* x, int ldx, int tf32, int* err,
+                                cudaStream_t st) {
+    if (n > 256 || ldx > 256 || T_total < 2) return cudaErrorInvalidValue;
+    double* part = nullptr;
+    cudaError_t e = cudaMallocAsync(&part, sizeof(double) * pp_part_len(T, n), st);
+    if (e != cudaSuccess) return e;
+    if (do_sphere != 0)
+        k_scale_scatter<<<(n * n + 255) / 256, 256, 0, st>>>(scatter, n, (double)T_total, cov,
+                                                             evwork + (size_t)n * n + n);
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = pp_finish(raw, T, n, do_sphere, means, cov, sphere, evwork, ldetS_dev, x, ldx, tf32, err, part,
+                      true, st, 0);
+    cudaFreeAsync(part, st);
+    return e;
 }
 
 cudaError_t launch_convert_sphered(const double* xs, int64_t T, int n, float* x, int ldx, int tf32,

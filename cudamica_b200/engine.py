@@ -43,7 +43,9 @@ EXPORTED = (
     "amica_last_cuda_error", "amica_set_iter_state", "amica_get_sphere", "amica_time_estep",
     "amica_launches_per_iteration", "amica_selftest_umma", "amica_estep_stats_noalloc",
     "amica_run_async", "amica_run_wait", "amica_set_grid", "amica_cohort_create",
-    "amica_cohort_run", "amica_cohort_destroy")
+    "amica_cohort_run", "amica_cohort_destroy", "amica_test_arm_wait_fault",
+    "amica_shard_estep", "amica_shard_mstep", "amica_shard_colsum", "amica_shard_scatter",
+    "amica_shard_sphere")
 
 
 class Cfg(C.Structure):
@@ -92,6 +94,12 @@ def lib():
         L.amica_run.argtypes = [vp, _i64, C.POINTER(IterOut)]
         L.amica_run_async.argtypes = [vp, _i64]
         L.amica_set_grid.argtypes = [vp, _i64, C.POINTER(_i64)]
+        L.amica_test_arm_wait_fault.argtypes = [vp, _i64]
+        L.amica_shard_estep.argtypes = [vp, vp]
+        L.amica_shard_mstep.argtypes = [vp, vp, _i64, C.POINTER(IterOut)]
+        L.amica_shard_colsum.argtypes = [vp, vp]
+        L.amica_shard_scatter.argtypes = [vp, vp, _i64, vp]
+        L.amica_shard_sphere.argtypes = [vp, vp, _i64]
         L.amica_run_wait.argtypes = [vp, C.POINTER(IterOut)]
         L.amica_cohort_create.argtypes = [C.POINTER(vp), _i64, C.POINTER(vp)]
         L.amica_cohort_run.argtypes = [vp, _i64, C.POINTER(IterOut), C.POINTER(_dbl)]
@@ -235,6 +243,43 @@ class Amica:
         outs = (IterOut * max(iters, 1))()
         _chk(lib().amica_run(self._ctx, iters, outs), "amica_run")
         return [outs[k] for k in range(iters)]
+
+    def shard_estep(self, d_stats: int) -> None:
+        """This shard's E-step statistics into device memory at d_stats
+        (stats_len doubles; amica_shard_estep)."""
+        _chk(lib().amica_shard_estep(self._ctx, C.c_void_p(d_stats)), "amica_shard_estep")
+
+    def shard_mstep(self, d_stats: int, nkeep_total: int) -> IterOut:
+        """The M-step from the statistics of all shards at d_stats (device;
+        amica_shard_mstep)."""
+        out = IterOut()
+        _chk(lib().amica_shard_mstep(self._ctx, C.c_void_p(d_stats), int(nkeep_total), C.byref(out)),
+             "amica_shard_mstep")
+        return out
+
+    def shard_colsum(self, d_sums: int) -> None:
+        """Column sums of this shard's raw data into device memory (n doubles)."""
+        _chk(lib().amica_shard_colsum(self._ctx, C.c_void_p(d_sums)), "amica_shard_colsum")
+
+    def shard_scatter(self, d_sums_total: int, T_total: int, d_scatter: int) -> None:
+        """Mean from the column sums of all shards; this shard's scatter about
+        it into device memory (n x n doubles)."""
+        _chk(lib().amica_shard_scatter(self._ctx, C.c_void_p(d_sums_total), int(T_total),
+                                       C.c_void_p(d_scatter)), "amica_shard_scatter")
+
+    def shard_sphere(self, d_scatter_total: int, T_total: int) -> None:
+        """Sphering from the scatter of all shards, applied to this shard."""
+        _chk(lib().amica_shard_sphere(self._ctx, C.c_void_p(d_scatter_total), int(T_total)),
+             "amica_shard_sphere")
+
+    @property
+    def stats_len(self) -> int:
+        return int(lib().amica_stats_len(self.n, self.M, self.m))
+
+    def arm_wait_fault(self, wait_cycles: int) -> None:
+        """Test hook: the next preprocess() has one missed grid-barrier arrival
+        and waits bounded by wait_cycles (amica_test_arm_wait_fault)."""
+        _chk(lib().amica_test_arm_wait_fault(self._ctx, int(wait_cycles)), "amica_test_arm_wait_fault")
 
     def set_grid(self, max_clusters: int) -> int:
         """Cap the E-step grid at max_clusters clusters (0: all that fit); returns

@@ -203,6 +203,50 @@ int64_t amica_launches_per_iteration(amica_ctx *ctx);
 int amica_selftest_umma(int mode, int N, int K, const float *A, const float *B, float *D,
                         int *device_err);
 
+/* Sample-sharded fits, one context per GPU, each over a contiguous range of
+ * the samples (its own load_data / set_sphered of T_shard samples, the same
+ * sphering and initial state on every shard).  Replaces the reference's
+ * multi-device block loop and its per-device statistics reduction
+ * (src/amica.cu:1618-1920, acumulate in src/kernels.cu:834-839).
+ * amica_shard_estep: the E-step over this context's samples; d_stats (DEVICE
+ * memory, amica_stats_len(n, M, m) doubles) receives its sufficient
+ * statistics, which are sums over samples, so that adding the vectors of all
+ * shards (one all-reduce) gives those of the whole data.
+ * amica_shard_mstep: the M-step from the added statistics d_stats (DEVICE),
+ * nkeep_total the samples of all shards; every shard runs it on the same
+ * vector, so the parameters stay identical across shards.  Both synchronise
+ * their stream.  Rejection needs every sample's P and is not available here
+ * (AMICA_ERR_UNSUPPORTED). */
+int amica_shard_estep(amica_ctx *ctx, double *d_stats);
+int amica_shard_mstep(amica_ctx *ctx, const double *d_stats, int64_t nkeep_total,
+                      amica_iter_out *out);
+
+/* Sharded preprocessing of raw data (after amica_load_data of this shard's
+ * samples), the GPU form of the reference's centring and sphering
+ * (src/preprocess.cu:31-230) over the samples of every shard, with two sums
+ * added across shards between the calls (DEVICE memory throughout):
+ * amica_shard_colsum: the column sums of this shard (n doubles);
+ * amica_shard_scatter: with the added sums of all shards and their sample
+ *   count T_total, sets the mean and writes this shard's scatter about it,
+ *   sum_t (x_t - mean)(x_t - mean)^T (n x n doubles);
+ * amica_shard_sphere: from the added scatter of all shards, the covariance,
+ *   its eigendecomposition, S and ldetS (the same on every shard), applied to
+ *   this shard's samples; the context is then ready for amica_init(). */
+int amica_shard_colsum(amica_ctx *ctx, double *d_sums);
+int amica_shard_scatter(amica_ctx *ctx, const double *d_sums_total, int64_t T_total,
+                        double *d_scatter);
+int amica_shard_sphere(amica_ctx *ctx, const double *d_scatter_total, int64_t T_total);
+
+/* Test hook for the failure path of the bounded device waits: arms the next
+ * amica_preprocess() of this context so that one block of its cooperative
+ * eigensolver (used above 128 channels with do_sphere = 1) skips its first
+ * grid-barrier arrival and every barrier wait of that launch gives up after
+ * wait_cycles clock cycles.  That amica_preprocess() then returns
+ * AMICA_ERR_TIMEOUT, and the context stays usable (the next one succeeds).
+ * No counterpart in the reference, whose waits are host synchronisations.
+ * AMICA_ERR_UNSUPPORTED for contexts that do not use the cooperative solver. */
+int amica_test_arm_wait_fault(amica_ctx *ctx, int64_t wait_cycles);
+
 /* E-step sufficient statistics with no allocation at all, for callers that
  * cannot call cudaMalloc (code running inside another framework's memory pool,
  * or a process that forbids device allocations after start-up).  No

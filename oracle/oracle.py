@@ -202,6 +202,19 @@ class Oracle:
             raise RuntimeError(f"oracle estep failed: {rc}")
         return self.stats.copy()
 
+    def mstep(self, stats: np.ndarray, nkeep: int | None = None) -> float:
+        """The M-step from a statistics vector (e.g. the sum of several shards'
+        estep() vectors), normalised by nkeep samples (default: this oracle's)."""
+        if nkeep is not None:
+            self.st.nkeep = int(nkeep)
+        self.lrate_hist.append(self.st.lrate)
+        s = np.ascontiguousarray(stats, dtype=np.float64)
+        rc = self._L.amo_mstep(C.byref(self.cfg), C.byref(self.st), _p(s))
+        if rc != 0:
+            raise RuntimeError(f"oracle mstep failed: {rc}")
+        self.ll_hist.append(self.st.ll)
+        return self.st.ll
+
     def params(self) -> dict:
         return dict(A=self.A.copy(), c=self.c.copy(), alpha=self.alpha.copy(), mu=self.mu.copy(),
                     beta=self.beta.copy(), rho=self.rho.copy(), gm=self.gm.copy(),

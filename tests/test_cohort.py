@@ -136,3 +136,30 @@ def test_persistent_cohort_matches_subjects_fitted_alone():
         assert np.max(np.abs(pa["A"] - pc["A"])) / np.max(np.abs(pa["A"])) < 1e-2, s
         eng.close()
     coh.close()
+
+
+@pytest.mark.gpu
+def test_persistent_cohort_first_iteration_against_oracle():
+    """Each subject of a persistent cohort (one E-step launch over all
+    subjects' tiles; n = 32, 64 and 128, i.e. lane packings R = 4, 2, 1)
+    against the FP64 oracle on its own data: the first iteration's LL (at the
+    deterministic start, identical parameters) within the mixed form's 1e-5
+    nats per sample and channel, the second within 2e-4 (one M-step of FP32
+    statistics on TF32-rounded data in between)."""
+    from cudamica_b200.cohort import Cohort
+    from oracle import oracle as O
+    specs = [(32, 20000, 11), (64, 30000, 12), (128, 25000, 13)]
+    data, inits = [], []
+    for n, T, seed in specs:
+        data.append(synth.config1(seed=seed, n=n, T=T, outlier_frac=0.0).x.astype(np.float32))
+        inits.append(synth.norand_init(n, 1))
+    coh = Cohort(data, M=1, m=3, precision=1, inits=inits, persistent=True)
+    outs = coh.run(2)
+    for s, (x, (A0, c0)) in enumerate(zip(data, inits)):
+        xs, _, _, ldetS = O.preprocess(x, 1)
+        orc = O.Oracle(xs, 1, 3, A0, c0, ldetS, nthreads=8)
+        lls = [orc.step(), orc.step()]
+        d = [abs(outs[s][k].ll - lls[k]) for k in range(2)]
+        print(f"subject {s} (n={x.shape[1]}): |dLL| {d[0]:.2e} {d[1]:.2e}")
+        assert d[0] < 1e-5 and d[1] < 2e-4, (s, d)
+    coh.close()
