@@ -528,7 +528,7 @@ def sharded_arm(args, ws: int, rank: int, local: int):
     eng, fit = fit_setup(xs)
     for _ in range(args.warmup):
         fit.step()
-    st = torch.cuda.current_stream(dev)
+    st = fit.shard.torch_stream                 # the engine's stream, where the iteration runs
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     dist.barrier()
     torch.cuda.synchronize()
@@ -543,10 +543,11 @@ def sharded_arm(args, ws: int, rank: int, local: int):
     # the exchange alone: the statistics all-reduce, 20 times
     a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     dist.barrier()
-    a0.record(st)
-    for _ in range(20):
-        dist.all_reduce(fit.buf, op=dist.ReduceOp.SUM)
-    a1.record(st)
+    with fit.shard.stream():
+        a0.record(st)
+        for _ in range(20):
+            dist.all_reduce(fit.buf, op=dist.ReduceOp.SUM)
+        a1.record(st)
     torch.cuda.synchronize()
     ar_ms = a0.elapsed_time(a1) / 20
     kernel, lpi = eng.kernel, eng.launches_per_iteration
@@ -600,6 +601,8 @@ def main():
     ap.add_argument("--fit-iters", type=int, default=1000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--sharded", action="store_true",
+                    help="the sample-sharded fit also on one rank (a one-member process group)")
     ap.add_argument("--replicas", action="store_true",
                     help="with N > 1 GPUs: N independent fits instead of one sample-sharded fit")
     ap.add_argument("--profile-case", action="store_true",
@@ -665,7 +668,16 @@ def main():
         print(json.dumps(line))
         return 0
 
-    if ws > 1 and not args.replicas:
+    if (ws > 1 and not args.replicas) or args.sharded:
+        if pg is None:                          # --sharded on one rank: a one-member group
+            import datetime
+            import torch
+            import torch.distributed as dist
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            os.environ.setdefault("MASTER_PORT", "29533")
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=600))
+            pg = dist
         out = sharded_arm(args, ws, rank, local)
         if rank == 0:
             print(json.dumps(out))

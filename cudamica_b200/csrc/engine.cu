@@ -1009,9 +1009,16 @@ int amica_shard_estep(amica_ctx* c, double* d_stats) {
     TRY(enqueue_estep(c));
     CK(cudaMemcpyAsync(d_stats, c->b.stats, sizeof(double) * amica_stats_len(c->n, c->M, c->m),
                        cudaMemcpyDeviceToDevice, c->st));
-    CK(cudaStreamSynchronize(c->st));
+    // stream-ordered: the all-reduce that follows is queued behind it on this
+    // stream; a device error surfaces in amica_shard_mstep
     c->have_estep = true;
-    return check_device_error(c);
+    return AMICA_OK;
+}
+
+int amica_get_stream(amica_ctx* c, void** stream) {
+    if (!c || !stream) return AMICA_ERR_INVALIDPARAM;
+    *stream = (void*)c->st;
+    return AMICA_OK;
 }
 
 int amica_shard_mstep(amica_ctx* c, const double* d_stats, int64_t nkeep_total, amica_iter_out* out) {

@@ -45,7 +45,7 @@ EXPORTED = (
     "amica_run_async", "amica_run_wait", "amica_set_grid", "amica_cohort_create",
     "amica_cohort_run", "amica_cohort_destroy", "amica_test_arm_wait_fault",
     "amica_shard_estep", "amica_shard_mstep", "amica_shard_colsum", "amica_shard_scatter",
-    "amica_shard_sphere")
+    "amica_shard_sphere", "amica_get_stream")
 
 
 class Cfg(C.Structure):
@@ -98,6 +98,7 @@ def lib():
         L.amica_shard_estep.argtypes = [vp, vp]
         L.amica_shard_mstep.argtypes = [vp, vp, _i64, C.POINTER(IterOut)]
         L.amica_shard_colsum.argtypes = [vp, vp]
+        L.amica_get_stream.argtypes = [vp, C.POINTER(vp)]
         L.amica_shard_scatter.argtypes = [vp, vp, _i64, vp]
         L.amica_shard_sphere.argtypes = [vp, vp, _i64]
         L.amica_run_wait.argtypes = [vp, C.POINTER(IterOut)]
@@ -246,7 +247,7 @@ class Amica:
 
     def shard_estep(self, d_stats: int) -> None:
         """This shard's E-step statistics into device memory at d_stats
-        (stats_len doubles; amica_shard_estep)."""
+        (stats_len doubles; amica_shard_estep), queued on self.stream."""
         _chk(lib().amica_shard_estep(self._ctx, C.c_void_p(d_stats)), "amica_shard_estep")
 
     def shard_mstep(self, d_stats: int, nkeep_total: int) -> IterOut:
@@ -256,6 +257,13 @@ class Amica:
         _chk(lib().amica_shard_mstep(self._ctx, C.c_void_p(d_stats), int(nkeep_total), C.byref(out)),
              "amica_shard_mstep")
         return out
+
+    @property
+    def stream(self) -> int:
+        """The context's cudaStream_t, as an integer handle."""
+        h = C.c_void_p()
+        _chk(lib().amica_get_stream(self._ctx, C.byref(h)), "amica_get_stream")
+        return int(h.value or 0)
 
     def shard_colsum(self, d_sums: int) -> None:
         """Column sums of this shard's raw data into device memory (n doubles)."""

