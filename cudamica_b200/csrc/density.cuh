@@ -257,17 +257,18 @@ __device__ __forceinline__ float2 tc_lse_pair(const float2* q) {
 }
 
 // Phase 2 for two samples of one mixture: from b, the kept L2 and the
-// per-sample -lse and v, q2 = 2^((rho-2) L2) and the responsibility
+// per-sample lse and v, q2 = 2^((rho-2) L2) and the responsibility
 // z = 2^(q - lse) (two ex2 per element, no reciprocal), then the seven sums
-// (A0..A6 as in tc_phase2) and g.
-__device__ __forceinline__ void tcp2(const MixT2& P, float2 bx, float2 L2, float2 nlse, float2 v,
+// (A0..A6 as in tc_phase2) and g.  (q - lse is formed as fma(lse, -1, q):
+// exact negation, one rounding, the same value as q + (-lse).)
+__device__ __forceinline__ void tcp2(const MixT2& P, float2 bx, float2 L2, float2 lse, float2 v,
                                      float2* A, float2& g) {
     const float2 y = __ffma2_rn(P.s, bx, P.npo);
     const float2 e = __fmul2_rn(P.pm2, L2);
     const float2 q2 = make_float2(ptx_ex2(e.x), ptx_ex2(e.y));
     const float2 y2 = __fmul2_rn(y, y);
     const float2 p = __fmul2_rn(q2, y2);
-    const float2 t = __fadd2_rn(__ffma2_rn(f2s(-kLog2e), p, P.pc), nlse);
+    const float2 t = __ffma2_rn(lse, f2s(-1.f), __ffma2_rn(f2s(-kLog2e), p, P.pc));
     const float2 z = make_float2(ptx_ex2(t.x), ptx_ex2(t.y));
     const float2 u = __fmul2_rn(v, z);
     const float2 w = __fmul2_rn(u, q2);

@@ -42,6 +42,11 @@ using namespace amica;
 
 namespace {
 
+template <int V>
+struct IntC {
+    static constexpr int value = V;
+};
+
 constexpr int kS = 48;                  // samples per tile (MMA1 N)
 constexpr int kWG = 3;                  // density warpgroups
 constexpr int kDensWarps = 4 * kWG;     // 12
@@ -68,26 +73,26 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
 }
-// try_wait with a suspend-time hint: a waiting thread sleeps until the phase
-// completes or the hint (ns) runs out, instead of spinning on issue slots the
-// density warps need.
-constexpr uint32_t kSuspendNs = 20000;
+// try_wait without a suspend-time hint: the waiting thread is suspended for a
+// system-dependent time or until the phase completes.  Measured at n=128,
+// T=1M, M=3, m=3: 3.05 ms per E-step, against 3.23 ms with a 20 us hint,
+// 3.22 ms with 1 us and 3.11 ms with 0.
 __device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok) : "r"(addr), "r"(parity), "n"(kSuspendNs) : "memory");
+        : "=r"(ok) : "r"(addr), "r"(parity) : "memory");
     return ok != 0;
 }
 __device__ __forceinline__ bool mbar_try_cluster(uint32_t addr, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok) : "r"(addr), "r"(parity), "n"(kSuspendNs) : "memory");
+        : "=r"(ok) : "r"(addr), "r"(parity) : "memory");
     return ok != 0;
 }
 // the CTA's abort flag, read and written as shared memory
@@ -294,10 +299,13 @@ struct TcShape {
     // per-warp channel sums of Lt from every model's CTA: [2][8 models][4 warps][kS] f32
     static constexpr uint32_t OFF_SLOT = OFF_BT + G_BYTES;
     static constexpr uint32_t OFF_LSE = OFF_SLOT + 2 * kMaxModels * 4 * kS * 4;  // [WG][kSub][128] f32
-    static constexpr uint32_t OFF_BAR = OFF_LSE + kWG * kSub * 128 * 4;
+    static constexpr uint32_t OFF_V = OFF_LSE + kWG * kSub * 128 * 4;       // [warp][kSub] f32
+    static constexpr uint32_t OFF_BAR = OFF_V + kDensWarps * kSub * 4;
     static constexpr uint32_t NBAR = 32;
     static constexpr uint32_t OFF_MISC = OFF_BAR + NBAR * 8;
-    static constexpr uint32_t BYTES = OFF_MISC + 64;
+    // per density warp: the models' log-likelihood offsets ltc_q - ltc_0 (FP32)
+    static constexpr uint32_t OFF_LC = OFF_MISC + 64;
+    static constexpr uint32_t BYTES = OFF_LC + kDensWarps * kMaxModels * 4;
     static constexpr uint32_t TMEM_COLS = 512;   // b: [0,48) [64,112); phi: [128,128+NP); W_lo: [256,256+NP);
                                                  // log2|y| cache: [48,64) [112,128) [384,512)
     static_assert(BYTES + 1024 <= 232448, "shared memory");
@@ -330,8 +338,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     // not change); the one that does not match the flag leaves at once.
     if ((a.split_phi != nullptr && *a.split_phi != 0) != SPLIT) return;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    // 1024-byte alignment for the swizzled operand tiles
-    uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    // 1024-byte alignment for the swizzled operand tiles (pointer arithmetic on
+    // the shared array, so that every pointer derived from it stays a shared
+    // memory pointer and its accesses compile to shared loads and stores)
+    uint8_t* sm = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     float* Wsm = (float*)(sm + Sh::OFF_W);
     float* slot = (float*)(sm + Sh::OFF_SLOT);
     uint64_t* bar = (uint64_t*)(sm + Sh::OFF_BAR);
@@ -497,7 +507,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     constexpr bool SPLIT = false;
     using Sh = TcShape<NP>;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* sm = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     uint64_t* bar = (uint64_t*)(sm + Sh::OFF_BAR);
     uint32_t* tmem_holder = (uint32_t*)(sm + Sh::OFF_MISC);
     volatile int* abort_flag = (volatile int*)(sm + Sh::OFF_MISC + 8);
@@ -605,7 +615,7 @@ __global__ void __launch_bounds__(128, 1) umma_selftest_kernel(const float* __re
                                                                float* __restrict__ D, int mode,
                                                                int N, int K, int* err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* sm = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     uint8_t* As = sm;                      // K-major, 128 rows, ceil(K/32) blocks of 16 KB
     uint8_t* Bs = sm + 2 * 16384;          // K-major, N rows
     uint64_t* bar = (uint64_t*)(sm + 2 * 16384 + 2 * 16384);
