@@ -11,7 +11,6 @@ from __future__ import annotations
 import argparse
 import concurrent.futures as cf
 import os
-import shutil
 import subprocess
 import sys
 
@@ -25,13 +24,8 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
-# cuBLAS (the split mixed form's TF32 GEMMs above 128 channels), found at run
-# time through the toolkit's library directory
-_CUDA_LIB = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(
-    shutil.which(NVCC) or "/usr/local/cuda/bin/nvcc"))), "lib64")
-CUBLAS = ["-L" + _CUDA_LIB, "-lcublas", "-Xlinker", "-rpath=" + _CUDA_LIB]
-SOURCES = ["engine.cu", "mstep.cu", "estep_plain.cu", "estep_tc.cu", "preprocess.cu", "adjoint.cu",
-           "estep_noalloc.cu"]
+SOURCES = ["engine.cu", "mstep.cu", "estep_plain.cu", "estep_tc.cu", "gemm_tc.cu", "preprocess.cu",
+           "adjoint.cu", "estep_noalloc.cu"]
 
 
 def _compile(src: str, verbose: bool) -> str:
@@ -59,7 +53,7 @@ def build(verbose: bool = False, cli: bool = True) -> str:
     with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), SOURCES))
     if (not os.path.exists(LIB)) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        cmd = [NVCC, *ARCH, "-shared", "--cudart=static", "-o", LIB, *objs, *CUBLAS]
+        cmd = [NVCC, *ARCH, "-shared", "--cudart=static", "-o", LIB, *objs]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

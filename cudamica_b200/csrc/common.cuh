@@ -109,8 +109,11 @@ struct EStepArgs {
     int ntiles, nclusters;
     int update_rho;
     int grad_mode;           // 1: beta-denominator slot holds sum u*f'*y for every rho (adjoint)
-    // density-only form (contractions done outside the kernel): b = W x and g
-    // per sample, both [T][M][NP] with a row of ldb floats per sample
+    // density-only form (contractions done outside the kernel): b = W x per
+    // sample, [T][M][NP] with a row of ldb floats per sample; g written as the
+    // operand image of the Psi contraction: per 32-sample block, model and
+    // 128-channel half, a 128 x 32 K-major tile with the 128-byte swizzle
+    // ([block][model][half][4096 floats], see sw128_off)
     const float* bext;
     float* gout;
     int ldb;

@@ -22,7 +22,6 @@
 #include <string>
 #include <vector>
 
-#include <cublas_v2.h>
 
 #include "amica_b200.h"
 #include "common.cuh"
@@ -38,7 +37,12 @@ bool plain_ext_supported(int n);
 int plain_ext_max_clusters(int m, int M);
 cudaError_t launch_estep_plain_ext(const EStepArgs& a, int nclusters, cudaStream_t st);
 cudaError_t launch_split_w(const float* Wf, float* whi, float* wlo, int64_t len, cudaStream_t st);
-cudaError_t launch_psi_add(const float* psi32, double* partial, int n, int m, int M, cudaStream_t st);
+// gemm_tc.cu
+cudaError_t launch_wx_tc(const float* x, int64_t T, const float* Whi, const float* Wlo, float* B, int M,
+                         int* err, cudaStream_t st);
+cudaError_t launch_gx_tc(const float* gimg, const float* ximg, int64_t T, int n, int m, int M, double* partial,
+                         int nslots, int* err, cudaStream_t st);
+cudaError_t launch_xt_image(const float* x, int64_t T, float* ximg, cudaStream_t st);
 // estep_tc.cu
 int tc_supported(int n, int m, int M);
 int tc_max_clusters(int n, int m, int M);
@@ -94,11 +98,9 @@ struct amica_ctx {
     bool use_tc = false;
     // split mixed form (128 < n <= 256): TF32 GEMMs around the density-only E-step
     bool use_split = false;
-    cublasHandle_t cublas = nullptr;
-    void* cublas_ws = nullptr;                    // the handle's workspace (graph capture)
     float *d_B = nullptr, *d_G = nullptr;         // T x M x NP: b = W x and g per sample
     float *d_Whi = nullptr, *d_Wlo = nullptr;     // M x NP x NP TF32 split of W
-    float* d_psi32 = nullptr;                     // M x n x n: one sample chunk of Psi
+    float* d_xT = nullptr;                        // x^T operand image of the Psi contraction
     int adj_nclusters = 0;                        // grid of the plain gradient kernel (split form)
     int nclusters = 0, ntiles = 0, nslots = 0;   // nslots: partial-sum slots per model
     int nclusters_cap = 0;                        // grid the partial-sum buffer was sized for
@@ -225,40 +227,27 @@ EStepArgs estep_args(amica_ctx* c) {
     return a;
 }
 
-// Samples per Psi GEMM: each chunk is summed in FP32 on the tensor cores and
-// added into the FP64 partial sums.
-constexpr int64_t kPsiChunk = 262144;
-
-#define CB(x)                                                                       \
-    do {                                                                            \
-        if ((x) != CUBLAS_STATUS_SUCCESS) return AMICA_ERR_CUDA;                    \
-    } while (0)
-
-// The split form's E-step: W -> (W_hi, W_lo), b = W_hi x + W_lo x, the
-// density-only kernel, Psi = sum g x^T per chunk of samples (TF32 GEMMs with
-// FP32 accumulation; W_hi has no bits below TF32, so only W_lo and the data
-// are rounded).
+// The split form's E-step: W -> (W_hi, W_lo), b = W_hi x + W_lo x (tensor-core
+// kernel), the density-only kernel, Psi = sum g x^T (tensor-core kernel, FP32
+// accumulation over at most 8192 samples, added into the partial slots in
+// FP64).  W_hi has no bits below TF32 and x and g are stored rounded to TF32,
+// so only W_lo is rounded by the MMA.
 int enqueue_split_estep(amica_ctx* c, const EStepArgs& a) {
-    const int M = c->M, NP = c->NP, n = c->n;
-    const int T = (int)c->T;
-    const float one = 1.f, zero = 0.f;
+    const int M = c->M, NP = c->NP;
     CK(launch_split_w(c->b.Wf, c->d_Whi, c->d_Wlo, (int64_t)M * NP * NP, c->st));
-    CB(cublasGemmEx(c->cublas, CUBLAS_OP_T, CUBLAS_OP_N, M * NP, T, NP, &one, c->d_Whi, CUDA_R_32F, NP,
-                    c->d_x, CUDA_R_32F, NP, &zero, c->d_B, CUDA_R_32F, M * NP,
-                    CUBLAS_COMPUTE_32F_FAST_TF32, CUBLAS_GEMM_DEFAULT));
-    CB(cublasGemmEx(c->cublas, CUBLAS_OP_T, CUBLAS_OP_N, M * NP, T, NP, &one, c->d_Wlo, CUDA_R_32F, NP,
-                    c->d_x, CUDA_R_32F, NP, &one, c->d_B, CUDA_R_32F, M * NP,
-                    CUBLAS_COMPUTE_32F_FAST_TF32, CUBLAS_GEMM_DEFAULT));
+    CK(launch_wx_tc(c->d_x, c->T, c->d_Whi, c->d_Wlo, c->d_B, M, c->b.err, c->st));
     CK(launch_estep_plain_ext(a, c->nclusters, c->st));
-    for (int64_t t0 = 0; t0 < c->T; t0 += kPsiChunk) {
-        const int k = (int)std::min<int64_t>(kPsiChunk, c->T - t0);
-        CB(cublasGemmStridedBatchedEx(c->cublas, CUBLAS_OP_N, CUBLAS_OP_T, n, n, k, &one,
-                                      c->d_G + t0 * (int64_t)M * NP, CUDA_R_32F, M * NP, NP,
-                                      c->d_x + t0 * NP, CUDA_R_32F, NP, 0, &zero, c->d_psi32,
-                                      CUDA_R_32F, n, (long long)n * n, M, CUBLAS_COMPUTE_32F_FAST_TF32,
-                                      CUBLAS_GEMM_DEFAULT));
-        CK(launch_psi_add(c->d_psi32, c->b.partial, n, c->m, M, c->st));
+    CK(launch_gx_tc(c->d_G, c->d_xT, c->T, c->n, c->m, M, c->b.partial, c->nslots, c->b.err, c->st));
+    return AMICA_OK;
+}
+
+// The sphered data is in place: the split form also needs its x^T image.
+int x_ready(amica_ctx* c) {
+    if (c->use_split) {
+        CK(launch_xt_image(c->d_x, c->T, c->d_xT, c->st));
+        CK(cudaStreamSynchronize(c->st));
     }
+    c->have_x = true;
     return AMICA_OK;
 }
 
@@ -276,9 +265,8 @@ int enqueue_estep(amica_ctx* c) {
 // (+ phi from Psi in the plain form), params, ctrl, A update (when A is
 // updated), reparametrisation, the finiteness check (+ rejection when enabled).
 int launches_per_iteration(const amica_ctx* c) {
-    // the split form adds the W split and one Psi add per sample chunk (its
-    // GEMMs are library kernels and not counted)
-    const int split = c->use_split ? 1 + (int)((c->T + kPsiChunk - 1) / kPsiChunk) : 0;
+    // the split form adds the W split and its two tensor-core contractions
+    const int split = c->use_split ? 3 : 0;
     return 8 + split + (c->hc.psi_is_phi ? 0 : 1) + (c->hc.update_A ? 1 : 0) + (c->hc.do_reject ? 1 : 0);
 }
 
@@ -487,17 +475,10 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     c->backup_len = param_len(c) + (sizeof(Ctrl) + 7) / 8;
     AL(c->d_backup, c->backup_len);
     if (c->use_split) {
-        AL(c->d_B, (size_t)T * M * NP); AL(c->d_G, (size_t)T * M * NP);
+        // g is written per 64-sample tile as the Psi operand image
+        AL(c->d_B, (size_t)T * M * NP); AL(c->d_G, (size_t)((T + 63) / 64) * 64 * M * NP);
+        AL(c->d_xT, (size_t)((T + 31) / 32) * 32 * NP);
         AL(c->d_Whi, (size_t)M * NP * NP); AL(c->d_Wlo, (size_t)M * NP * NP);
-        AL(c->d_psi32, (size_t)M * nn);
-        const size_t ws = (size_t)32 << 20;
-        if (cudaMalloc(&c->cublas_ws, ws) != cudaSuccess) { amica_destroy(c); return AMICA_ERR_CUDA; }
-        if (cublasCreate(&c->cublas) != CUBLAS_STATUS_SUCCESS ||
-            cublasSetStream(c->cublas, c->st) != CUBLAS_STATUS_SUCCESS ||
-            cublasSetWorkspace(c->cublas, c->cublas_ws, ws) != CUBLAS_STATUS_SUCCESS) {
-            amica_destroy(c);
-            return AMICA_ERR_CUDA;
-        }
     }
 #undef AL
     CK(cudaMemsetAsync(c->d_keep, 1, T, c->st));
@@ -518,9 +499,7 @@ int amica_destroy(amica_ctx* c) {
                     c->b.work, c->b.chunk, c->b.gj, c->b.bflag, c->b.use_newton, c->b.Wf, c->b.wcf,
                     c->b.mp, c->b.ctrl, c->b.hist, c->b.err, c->d_keep, c->d_Lt, c->d_P, c->d_x,
                     c->d_rawx, c->d_means, c->d_sphere, c->d_cov, c->d_evwork, c->d_ldetS,
-                    c->d_backup, c->d_gradp, c->d_grad, c->d_B, c->d_G, c->d_Whi, c->d_Wlo,
-                    c->d_psi32, c->cublas_ws};
-    if (c->cublas) cublasDestroy(c->cublas);
+                    c->d_backup, c->d_gradp, c->d_grad, c->d_B, c->d_G, c->d_Whi, c->d_Wlo, c->d_xT};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_ctrl) cudaFreeHost(c->h_ctrl);
@@ -571,7 +550,7 @@ int amica_preprocess(amica_ctx* c) {
     TRY(check_device_error(c));
     c->ldetS = ld;
     c->hc.ldetS = ld;
-    c->have_x = true;
+    TRY(x_ready(c));
     return AMICA_OK;
 }
 
@@ -590,7 +569,7 @@ int amica_set_sphered(amica_ctx* c, const double* xs, const double* means, const
     CK(cudaFree(tmp));
     c->ldetS = ldetS;
     c->hc.ldetS = ldetS;
-    c->have_x = true;
+    TRY(x_ready(c));
     return AMICA_OK;
 }
 
@@ -1088,7 +1067,7 @@ int amica_shard_sphere(amica_ctx* c, const double* d_scatter_total, int64_t T_to
     TRY(check_device_error(c));
     c->ldetS = ld;
     c->hc.ldetS = ld;
-    c->have_x = true;
+    TRY(x_ready(c));
     c->have_shard_mean = false;
     return AMICA_OK;
 }
@@ -1149,8 +1128,8 @@ int amica_time_estep(amica_ctx* c, int64_t reps, double* ms_per_launch, int64_t*
     CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     *ms_per_launch = (double)ms / (double)reps;
     // the constants' kernels, then (reps + 1) E-steps: the split form's E-step
-    // is the W split, the kernel and one Psi add per sample chunk
-    const int64_t per = c->use_split ? 2 + (c->T + kPsiChunk - 1) / kPsiChunk : 1;
+    // is the W split, b = W x, the density kernel and Psi = g x^T
+    const int64_t per = c->use_split ? 4 : 1;
     if (launches) *launches = (reps + 1) * per + 1;
     return AMICA_OK;
 }

@@ -28,6 +28,7 @@
 
 #include "common.cuh"
 #include "density.cuh"
+#include "tc_ptx.cuh"
 
 namespace cg = cooperative_groups;
 using namespace amica;
@@ -280,9 +281,8 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
                 fS1[k] = 0.f;
             }
             float fCn = 0.f, fS2 = 0.f, fGs = 0.f;
-#pragma unroll 2
-            for (int r = 0; r < Sh::SUB; r++) {
-                const int t = grp * Sh::SUB + r;
+            // the densities, responsibilities and sums of tile sample t; returns g
+            auto sample = [&](int t) -> float {
                 const float v = vS[t];
                 const float bx = bs[t * NPL + ch];
                 const float nl = -lse[t * Sh::LLD + ch];
@@ -297,11 +297,34 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
                 fCn = fmaf(v, bb, fCn);          // sum v b; cnew = A sum(v b) / vsum + c
                 fS2 = fmaf(v * bb, bb, fS2);
                 fGs += ch_ok ? g : 0.f;
-                if constexpr (EXT) {
-                    // stored as TF32 (round to nearest, ties away) so that the Psi GEMM reads it exactly
-                    const float gt = __uint_as_float((__float_as_uint(g) + 0x1000u) & 0xffffe000u);
-                    if (t0 + t < a.T) a.gout[(size_t)(t0 + t) * a.ldb + (size_t)h * NP + i0c + ch] = ch_ok ? gt : 0.f;
-                } else {
+                return g;
+            };
+            if constexpr (EXT) {
+                // g of four consecutive samples per 16-byte store into the
+                // operand image of the Psi contraction (row = channel within its
+                // 128-channel half, column = sample within its 32-sample block),
+                // stored as TF32 (round to nearest, ties away) so that the MMA
+                // reads it exactly; zero past T
+                const int rr = ch & 127, hc = ch >> 7;
+#pragma unroll 1
+                for (int r4 = 0; r4 < Sh::SUB; r4 += 4) {
+                    const int64_t tg = t0 + grp * Sh::SUB + r4;
+                    float gq[4];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const float g = sample(grp * Sh::SUB + r4 + q);
+                        const float gt = __uint_as_float((__float_as_uint(g) + 0x1000u) & 0xffffe000u);
+                        gq[q] = (ch_ok && tg + q < a.T) ? gt : 0.f;
+                    }
+                    float* dst = a.gout + (((size_t)(tg >> 5) * a.M + h) * 2 + hc) * 4096 +
+                                 sw128_off(rr, (int)(tg & 31), 128) / 4;
+                    *reinterpret_cast<float4*>(dst) = make_float4(gq[0], gq[1], gq[2], gq[3]);
+                }
+            } else {
+#pragma unroll 2
+                for (int r = 0; r < Sh::SUB; r++) {
+                    const int t = grp * Sh::SUB + r;
+                    const float g = sample(t);
                     gs[t * NPL + ch] = ch_ok ? g : 0.f;
                 }
             }
@@ -527,7 +550,7 @@ cudaError_t launch_estep_plain_ext(const EStepArgs& a, int nclusters, cudaStream
 namespace {
 
 // W_hi = tf32(W) (round to nearest, ties away: the low 13 bits zero, so the
-// GEMM's own TF32 conversion keeps it exactly) and W_lo = W - W_hi.
+// MMA's reading of it as TF32 keeps it exactly) and W_lo = W - W_hi.
 __global__ void k_split_w(const float* __restrict__ Wf, float* __restrict__ whi, float* __restrict__ wlo,
                           int64_t len) {
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < len; e += (int64_t)gridDim.x * blockDim.x) {
@@ -539,30 +562,12 @@ __global__ void k_split_w(const float* __restrict__ Wf, float* __restrict__ whi,
     }
 }
 
-// partial slot 0: Psi_h += the FP32 GEMM result of one sample chunk (n x n per model)
-__global__ void k_psi_add(const float* __restrict__ psi32, double* __restrict__ partial, int n, int M,
-                          int64_t stride, int psi_off) {
-    const int64_t nn = (int64_t)n * n;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < M * nn; e += (int64_t)gridDim.x * blockDim.x) {
-        const int h = (int)(e / nn);
-        partial[h * stride + psi_off + (e - h * nn)] += (double)psi32[e];
-    }
-}
-
 }  // namespace
 
 namespace amica {
 
 cudaError_t launch_split_w(const float* Wf, float* whi, float* wlo, int64_t len, cudaStream_t st) {
     k_split_w<<<(int)std::min<int64_t>((len + 255) / 256, 1184), 256, 0, st>>>(Wf, whi, wlo, len);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_psi_add(const float* psi32, double* partial, int n, int m, int M, cudaStream_t st) {
-    PartLayout L{n, m};
-    const int64_t len = (int64_t)M * n * n;
-    k_psi_add<<<(int)std::min<int64_t>((len + 255) / 256, 1184), 256, 0, st>>>(psi32, partial, n, M,
-                                                                               L.stride(), L.psi());
     return cudaGetLastError();
 }
 

@@ -94,8 +94,8 @@ int amica_default_cfg(amica_cfg *cfg);
  * (src/amica.cu:135-556).  Shapes: 2 <= nchannels <= 256, 1 <= nmmodels <= 8,
  * 1 <= nsdm <= 5 (else AMICA_ERR_UNSUPPORTED).  AMICA_PREC_MIXED runs the
  * fused tensor-core E-step up to 128 channels and, above, the split form:
- * b = W x and Psi = sum g x^T as TF32 tensor-core GEMMs (cuBLAS) around a
- * density-only E-step kernel.  amica_kernel_name() reports "tc_tf32",
+ * b = W x and Psi = sum g x^T as tcgen05 TF32 contraction kernels of this
+ * library around a density-only E-step kernel.  amica_kernel_name() reports "tc_tf32",
  * "split_tf32" or "plain_fp32". */
 int amica_create(const amica_cfg *cfg, amica_ctx **out);
 

@@ -140,19 +140,36 @@ def test_adjoint_vs_float64_autograd_and_differences(precision, c2_slice):
 
 
 def test_split_form_adjoint_above_128_channels():
-    """n = 160, M = 2: the mixed form above 128 channels (TF32 GEMMs around the
-    density-only kernel) computes its gradient with the plain gradient kernel
-    on its own grid, on the same buffers as its own E-step (which runs just
-    before); against float64 autograd on the stored data."""
+    """n = 160, M = 2: the mixed form above 128 channels (TF32 tensor-core
+    contractions around a density-only kernel) computes its gradient with the
+    plain gradient kernel on its own grid, on the same buffers as its own E-step
+    (which runs just before).  That gradient must equal, bit for bit, the one a
+    plain-form context computes at the same parameters on the same stored data,
+    and match float64 autograd there.  After three iterations from the
+    deterministic start the W and mu gradients are small (max |dW| ~3e-4, max
+    |dmu| ~5e-5 here), so their error relative to the largest entry is larger
+    than at n = 128: the band is 2e-3."""
+    from cudamica_b200.engine import Amica
     xs, means, S, ldetS = _slice(160, 2, T=20_000, full_T=200_000, seed=3)
     eng = _engine(xs, means, S, ldetS, 160, 2, 1)
     assert eng.kernel == "split_tf32"
+    p = eng.params()
     eng.estep_stats()                   # the split form's own E-step ran last
     ll_g, g_g = eng.adjoint()
-    ll_t, g_t, _, _ = _torch_ref(eng, _as_stored(xs, 1), ldetS, torch.device("cuda:0"))
+    stored = _as_stored(xs, 1)
+    ll_t, g_t, _, _ = _torch_ref(eng, stored, ldetS, torch.device("cuda:0"))
     errs = {k: _rel(g_g[k], g_t[k]) for k in ("W", "mu", "beta", "rho")}
     print(f"split form n=160: dLL {abs(ll_g - ll_t):.2e} " + " ".join(f"{k}={v:.2e}" for k, v in errs.items()))
     assert abs(ll_g - ll_t) < 2e-6
     for k, v in errs.items():
-        assert v < 2e-4, (k, v)
+        assert v < 2e-3, (k, v)
+    e0 = Amica(160, xs.shape[0], 2, 3, precision=0, update_rho=1)
+    e0.set_sphered(stored, means, S, ldetS)
+    e0.init(*synth.norand_init(160, 2))
+    e0.set_params(**{k: p[k] for k in ("A", "c", "gm", "alpha", "mu", "beta", "rho")})
+    ll0, g0 = e0.adjoint()
+    assert ll0 == ll_g
+    for k in g0:
+        assert np.array_equal(g0[k], g_g[k]), k
+    e0.close()
     eng.close()
