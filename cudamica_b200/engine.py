@@ -15,7 +15,8 @@ import os
 import numpy as np
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PKG, "libamica_b200.so")
+# the in-tree build; CUDAMICA_B200_LIB names another build of the same ABI
+LIB_PATH = os.environ.get("CUDAMICA_B200_LIB") or os.path.join(PKG, "libamica_b200.so")
 
 AMICA_PREC_FP32 = 0
 AMICA_PREC_MIXED = 1

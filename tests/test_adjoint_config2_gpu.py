@@ -16,13 +16,13 @@ and W gradients by ~2e-3 of their largest entries (the same data effect that
 moves the mu sums, test_parity_headline_gpu.py); its gradient is therefore
 checked against the reference on the data as it stores it, and its distance
 from the exact-data gradient is printed.  Bands, relative to the largest entry
-of each gradient: 2e-4 (plain) and 1e-3 (mixed: measured 4.6e-4; dW and dmu
-are differences of nearly cancelling terms near the optimum, vsum W^-T - phi A^T
-and sqrt(beta) sum u f', so phi's FP32-level error shows there amplified);
-finite differences: the largest gap within 1e-3 / 2e-3 of the gradient's scale
-and the median within 1e-4 / 2e-4, the exact float64 gradient itself meeting
-1e-3 and 1e-4 (the differences carry their own truncation error, largest on
-coordinates that move samples across the kink of |y|^rho at y = 0).
+of each gradient: 2e-4 (plain; measured 2.6e-5) and 5e-4 (mixed; measured
+7.9e-5: dW and dmu are differences of nearly cancelling terms, vsum W^-T -
+phi A^T and sqrt(beta) sum u f', so phi's FP32-level error shows there
+amplified); finite differences: the median gap within 1e-4 / 2e-4 of the
+gradient's scale and the largest within the float64 gradient's own largest
+gap plus the gradient band (the differences carry their own truncation error,
+largest on coordinates that move samples across the kink of |y|^rho at y = 0).
 """
 import numpy as np
 import pytest
@@ -35,8 +35,8 @@ import torch_ll
 
 pytestmark = pytest.mark.gpu
 
-TOL = {0: dict(ll=1e-6, g=2e-4, fd_max=1e-3, fd_med=1e-4),
-       1: dict(ll=2e-6, g=1e-3, fd_max=2e-3, fd_med=2e-4)}
+TOL = {0: dict(ll=1e-6, g=2e-4, fd_med=1e-4),
+       1: dict(ll=2e-6, g=5e-4, fd_med=2e-4)}
 
 
 def _as_stored(xs, precision):
@@ -134,8 +134,13 @@ def test_adjoint_vs_float64_autograd_and_differences(precision, c2_slice):
     gap_t, gap_a = np.abs(tg - fd) / scale, np.abs(ad - fd) / scale
     print(f"precision={precision}: differences vs float64 gradient max {gap_t.max():.2e} "
           f"median {np.median(gap_t):.2e}; vs adjoint max {gap_a.max():.2e} median {np.median(gap_a):.2e}")
-    assert gap_t.max() < 1e-3 and np.median(gap_t) < 1e-4       # the reference itself
-    assert gap_a.max() < tol["fd_max"] and np.median(gap_a) < tol["fd_med"]
+    # the float64 gradient itself: the differences carry their own truncation
+    # error, largest on coordinates that move samples across the kink of
+    # |y|^rho at y = 0 (up to 1.5e-3 of the scale at some parameter points)
+    assert np.median(gap_t) < 1e-4 and gap_t.max() < 2e-3
+    # the adjoint: as close to the differences as the float64 gradient, up to
+    # its own gradient band
+    assert np.median(gap_a) < tol["fd_med"] and gap_a.max() < gap_t.max() + tol["g"]
     eng.close()
 
 
