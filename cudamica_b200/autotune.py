@@ -1,13 +1,23 @@
-"""Launch-shape autotuning for the fused E-step.
+"""Measured choice of the fused E-step's tile shape and launch shape.
 
-The E-step kernels are persistent: one cluster of M CTAs (one CTA per SM) per
-stream of sample tiles, as many clusters as fit by default.  What is tunable
-per problem shape is how many clusters a context runs -- alone on the GPU the
-fastest grid, inside a cohort of contexts that run concurrently the split of
-the SMs between subjects (or none: every subject on the whole GPU, their
-streams interleaving).  Both are chosen from measurements (amica_time_estep for
-one context, timed cohort iterations for a cohort); results are cached per
-shape for the process, and optionally in a JSON file.
+The fused mixed-form E-step (up to 128 channels) is compiled in three tile
+shapes (amica_cfg.tc_shape): 0 = 3 density warpgroups and 48-sample tiles with
+2 TMA stages of x, 1 = 2 warpgroups and 32-sample tiles with 2 stages, 2 = 2
+warpgroups with 3 stages.  The shape sets the samples per tile (MMA1 N, MMA2
+K), the density warps per SM and the x pipeline depth; the fastest depends on
+n (lane packing), M (cluster size) and m (registers and tensor-memory
+columns for the log2|y| cache), so best_tile_shape times each on the
+context's own data (the reference derives its launch shapes from n and the
+SM count instead, src/helpers.cu:55-511).
+
+The kernels are persistent: one cluster of M CTAs (one CTA per SM) per stream
+of sample tiles, as many clusters as fit by default.  Also tunable is how many
+clusters a context runs -- alone on the GPU the fastest grid, inside a cohort
+of contexts that run concurrently the split of the SMs between subjects (or
+none: every subject on the whole GPU, their streams interleaving).  All are
+chosen from measurements (amica_time_estep for one context, timed cohort
+iterations for a cohort); results are cached per problem shape for the
+process, and optionally in a JSON file.
 """
 from __future__ import annotations
 
@@ -45,6 +55,36 @@ def estep_profile(eng: Amica, grids: Iterable[int], reps: int = 5) -> dict:
         out[real] = ms
     eng.set_grid(0)
     return out
+
+
+TILE_SHAPES = (0, 1, 2)
+
+
+def tile_shape_profile(eng: Amica, reps: int = 5) -> dict:
+    """E-step ms of the context in each tile shape on its own data and
+    parameters (full grid).  Leaves the context in shape 0."""
+    out = {}
+    for sh in TILE_SHAPES:
+        eng.set_tile_shape(sh)
+        eng.estep_stats()                     # first launch of this shape, untimed
+        out[sh] = eng.time_estep(reps)[0]
+    eng.set_tile_shape(0)
+    return out
+
+
+def best_tile_shape(eng: Amica, reps: int = 5) -> int:
+    """The fastest tile shape for the context's (n, T, M, m), measured once
+    per problem shape and cached; the context is left in it.  Contexts that
+    do not run the fused form keep their kernel (returns -1)."""
+    if eng.kernel != "tc_tf32":
+        return -1
+    key = "tile:" + _key(eng)
+    if key not in _cache:
+        prof = tile_shape_profile(eng, reps)
+        _cache[key] = {"best": min(prof, key=prof.get), "ms": {str(k): v for k, v in prof.items()}}
+    best = int(_cache[key]["best"])
+    eng.set_tile_shape(best)
+    return best
 
 
 def best_grid(eng: Amica, tolerance: float = 0.03, reps: int = 5) -> int:

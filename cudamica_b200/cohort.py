@@ -10,9 +10,10 @@ own CUDA stream.  Two ways to advance them:
   (engine.PersistentCohort, amica_cohort_*);
 * streams: one graph replay per subject, all enqueued before any is waited
   for, so the subjects' E-steps and their small M-step kernels overlap.  The
-  autotuner times a few cohort iterations with every subject on the whole GPU
-  and with the SMs split in proportion to each subject's E-step work, keeps
-  the faster, and restores the starting state.
+  autotuner puts each subject's fused E-step in its fastest tile shape
+  (autotune.best_tile_shape), then times a few cohort iterations with every
+  subject on the whole GPU and with the SMs split in proportion to each
+  subject's E-step work, keeps the faster, and restores the starting state.
 """
 from __future__ import annotations
 
@@ -49,6 +50,9 @@ class Cohort:
             import torch
             sm_budget = torch.cuda.get_device_properties(device).multi_processor_count
         self.timings = {}
+        # each subject's fused E-step in its fastest tile shape (the persistent
+        # kernel above runs one shape for all subjects)
+        self.tile_shapes = [autotune.best_tile_shape(e) if tune else 0 for e in self.engines]
         if grids is not None:
             self.grids = list(grids)
         elif tune:

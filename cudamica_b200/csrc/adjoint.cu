@@ -22,7 +22,7 @@
 
 namespace amica {
 cudaError_t launch_estep_plain(const EStepArgs& a, int NP, int nclusters, cudaStream_t st);
-cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStream_t st, int split);
+cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStream_t st, int split, int shape);
 }
 
 using namespace amica;
@@ -96,13 +96,13 @@ namespace amica {
 
 // The adjoint sweep: the fused E-step in gradient mode into `partial`.
 cudaError_t launch_adjoint(const EStepArgs& a0, int NP, double* grad_partial, int nclusters,
-                           cudaStream_t st, bool use_tc) {
+                           cudaStream_t st, bool use_tc, int tc_shape) {
     EStepArgs a = a0;
     a.grad_mode = 1;
     a.update_rho = 1;
     a.partial = grad_partial;
     a.split_phi = nullptr;   // the gradient sweep does not need phi's split correction
-    return use_tc ? launch_estep_tc(a, NP, nclusters, st, 0) : launch_estep_plain(a, NP, nclusters, st);
+    return use_tc ? launch_estep_tc(a, NP, nclusters, st, 0, tc_shape) : launch_estep_plain(a, NP, nclusters, st);
 }
 
 cudaError_t launch_adjoint_finalize(const double* grad_partial, double* raw, int nclusters, int n,

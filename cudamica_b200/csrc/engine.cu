@@ -45,16 +45,17 @@ cudaError_t launch_gx_tc(const float* gimg, const float* ximg, int64_t T, int n,
 cudaError_t launch_xt_image(const float* x, int64_t T, float* ximg, cudaStream_t st);
 // estep_tc.cu
 int tc_supported(int n, int m, int M);
-int tc_max_clusters(int n, int m, int M);
-int tc_tile_samples(int n);
-int tc_partial_groups(int n);
-int tc_psi_step();
+int tc_max_clusters(int n, int m, int M, int shape);
+int tc_tile_samples(int n, int shape);
+int tc_partial_groups(int n, int shape);
+int tc_psi_step(int shape);
+int tc_num_shapes();
 int tc_cohort_encode_map(const EStepArgs& a, void* map);
 int tc_cohort_ctas();
 cudaError_t launch_estep_tc_cohort(const TcCohortSub* subs, const void* maps, const TcCohortItem* items,
                                    const int* item_off, int nctas, int m, cudaStream_t st);
 int tc_selftest(int mode, int N, int K, const float* hA, const float* hB, float* hD, int* derr);
-cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStream_t st, int split);
+cudaError_t launch_estep_tc(const EStepArgs& a, int NP, int nclusters, cudaStream_t st, int split, int shape);
 // preprocess.cu
 cudaError_t launch_preprocess(const float* raw, int64_t T, int n, int do_sphere, double* means,
                               double* cov, double* sphere, double* evwork, double* ldetS_dev,
@@ -71,7 +72,7 @@ cudaError_t launch_shard_finish(const float* raw, int64_t T, int n, int do_spher
                                 cudaStream_t st);
 // adjoint.cu
 cudaError_t launch_adjoint(const EStepArgs& a, int NP, double* grad_partial, int nclusters,
-                           cudaStream_t st, bool use_tc);
+                           cudaStream_t st, bool use_tc, int tc_shape);
 cudaError_t launch_adjoint_finalize(const double* grad_partial, double* raw, int nclusters, int n,
                                     int m, int M, const double* A, const double* c,
                                     const double* beta, const double* rho, double* out,
@@ -103,6 +104,7 @@ struct amica_ctx {
     float* d_xT = nullptr;                        // x^T operand image of the Psi contraction
     int adj_nclusters = 0;                        // grid of the plain gradient kernel (split form)
     int nclusters = 0, ntiles = 0, nslots = 0;   // nslots: partial-sum slots per model
+    int tc_shape = 0;                             // tile shape of the fused E-step
     int nclusters_cap = 0;                        // grid the partial-sum buffer was sized for
     bool have_data = false, have_x = false, have_init = false, have_estep = false;
     bool have_shard_mean = false;   // amica_shard_scatter has set the mean of all shards
@@ -255,7 +257,7 @@ int enqueue_estep(amica_ctx* c) {
     CK(launch_prep(c->b, c->hc, c->st));
     EStepArgs a = estep_args(c);
     if (c->use_split) TRY(enqueue_split_estep(c, a));
-    else if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st, c->hc.phi_split));
+    else if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st, c->hc.phi_split, c->tc_shape));
     else CK(launch_estep_plain(a, c->NP, c->nclusters, c->st));
     CK(launch_reduce_finalize(c->b, c->hc, c->nslots, c->st));
     return AMICA_OK;
@@ -341,6 +343,7 @@ int amica_default_cfg(amica_cfg* c) {
     c->seed = 1234;
     c->verbose = 0;
     c->phi_split = 2;
+    c->tc_shape = 0;
     c->phi_split_rel = kPhiSplitRel;
     c->lrate0 = 0.1;
     c->lratemax = 1.0;
@@ -405,15 +408,25 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     c->use_tc = (cfg->precision == AMICA_PREC_MIXED) && tc_supported((int)n, (int)m, (int)M);
     c->use_split = (cfg->precision == AMICA_PREC_MIXED) && !c->use_tc && plain_ext_supported((int)n) &&
                    T <= 0x7fffffff;
-    c->S = c->use_tc ? tc_tile_samples((int)n) : plain_tile_samples();
+    if (cfg->tc_shape < 0 || cfg->tc_shape >= tc_num_shapes()) { amica_destroy(c); return AMICA_ERR_INVALIDPARAM; }
+    c->tc_shape = c->use_tc ? (int)cfg->tc_shape : 0;
+    c->S = c->use_tc ? tc_tile_samples((int)n, c->tc_shape) : plain_tile_samples();
     c->ntiles = (int)((T + c->S - 1) / c->S);
-    int maxcl = c->use_tc      ? tc_max_clusters((int)n, (int)m, (int)M)
+    int maxcl = c->use_tc      ? tc_max_clusters((int)n, (int)m, (int)M, c->tc_shape)
                 : c->use_split ? plain_ext_max_clusters((int)m, (int)M)
                                : plain_max_clusters((int)n, (int)m, (int)M);
     if (maxcl <= 0) { amica_destroy(c); return AMICA_ERR_UNSUPPORTED; }
-    // partial-sum slots are sized for the full grid so that amica_set_grid can
-    // move between any grid sizes later
+    // partial-sum slots are sized for the full grid (and, in the fused form,
+    // every tile shape) so that amica_set_grid and amica_set_tile_shape can
+    // move between them later
     c->nclusters_cap = maxcl < c->ntiles ? maxcl : c->ntiles;
+    if (c->use_tc)
+        for (int sh = 0; sh < tc_num_shapes(); sh++) {
+            const int mc = tc_max_clusters((int)n, (int)m, (int)M, sh);
+            const int nt = (int)((T + tc_tile_samples((int)n, sh) - 1) / tc_tile_samples((int)n, sh));
+            const int cap = mc < nt ? mc : nt;
+            if (cap > c->nclusters_cap) c->nclusters_cap = cap;
+        }
     if (cfg->max_clusters > 0 && cfg->max_clusters < maxcl) maxcl = (int)cfg->max_clusters;
     c->nclusters = maxcl < c->ntiles ? maxcl : c->ntiles;
 
@@ -430,7 +443,7 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     h.rholrate = cfg->rholrate; h.rhomin = cfg->rhomin; h.rhomax = cfg->rhomax;
     h.rejsig = cfg->rejsig; h.ldetS = 0.0;
     h.psi_is_phi = c->use_tc ? 1 : 0;
-    h.psi_step = c->use_tc ? tc_psi_step() : 1;
+    h.psi_step = c->use_tc ? tc_psi_step(c->tc_shape) : 1;
     h.phi_split = c->use_tc ? (int)cfg->phi_split : 0;
     h.phi_split_rel = cfg->phi_split_rel;
 
@@ -442,9 +455,12 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     AL(b.beta, M * mn); AL(b.rho, M * mn); AL(b.gm, M); AL(b.W, M * nn); AL(b.ldet, M);
     AL(b.ltc64, M);
     PartLayout PL{(int)n, (int)m};
-    const int groups = c->use_tc ? tc_partial_groups((int)n) : c->use_split ? 1 : plain_partial_groups((int)n);
+    const int groups = c->use_tc ? tc_partial_groups((int)n, c->tc_shape) : c->use_split ? 1 : plain_partial_groups((int)n);
     c->nslots = c->nclusters * groups;
-    size_t pslots = (size_t)c->nclusters_cap * groups;
+    int gmax = groups;
+    if (c->use_tc)
+        for (int sh = 0; sh < tc_num_shapes(); sh++) gmax = std::max(gmax, tc_partial_groups((int)n, sh));
+    size_t pslots = (size_t)c->nclusters_cap * gmax;
     if (c->use_split) {
         // its adjoint runs the plain gradient kernel (channel-split clusters)
         const int pcl = plain_max_clusters((int)n, (int)m, (int)M);
@@ -728,7 +744,7 @@ int amica_set_grid(amica_ctx* c, int64_t max_clusters, int64_t* nclusters) {
     if (!c || max_clusters < 0) return AMICA_ERR_INVALIDPARAM;
     if (c->pending >= 0) return AMICA_ERR_STATE;
     CK(cudaSetDevice(c->dev));
-    int maxcl = c->use_tc      ? tc_max_clusters(c->n, c->m, c->M)
+    int maxcl = c->use_tc      ? tc_max_clusters(c->n, c->m, c->M, c->tc_shape)
                 : c->use_split ? plain_ext_max_clusters(c->m, c->M)
                                : plain_max_clusters(c->n, c->m, c->M);
     if (maxcl <= 0) return AMICA_ERR_UNSUPPORTED;
@@ -737,13 +753,38 @@ int amica_set_grid(amica_ctx* c, int64_t max_clusters, int64_t* nclusters) {
     // the partial-sum slots were sized for the largest grid at creation
     if (ncl > c->nclusters_cap) return AMICA_ERR_INVALIDPARAM;
     c->nclusters = ncl;
-    c->nslots = ncl * (c->use_tc ? tc_partial_groups(c->n) : c->use_split ? 1 : plain_partial_groups(c->n));
+    c->nslots = ncl * (c->use_tc ? tc_partial_groups(c->n, c->tc_shape) : c->use_split ? 1 : plain_partial_groups(c->n));
     if (c->graph) {
         CK(cudaStreamSynchronize(c->st));
         cudaGraphExecDestroy(c->graph);
         c->graph = nullptr;
     }
     if (nclusters) *nclusters = ncl;
+    return AMICA_OK;
+}
+
+int amica_set_tile_shape(amica_ctx* c, int64_t shape) {
+    if (!c || shape < 0 || shape >= tc_num_shapes()) return AMICA_ERR_INVALIDPARAM;
+    if (!c->use_tc) return AMICA_ERR_UNSUPPORTED;
+    if (c->pending >= 0) return AMICA_ERR_STATE;
+    CK(cudaSetDevice(c->dev));
+    const int S = tc_tile_samples(c->n, (int)shape);
+    const int ntiles = (int)((c->T + S - 1) / S);
+    const int mc = tc_max_clusters(c->n, c->m, c->M, (int)shape);
+    if (mc <= 0) return AMICA_ERR_UNSUPPORTED;
+    const int ncl = mc < ntiles ? mc : ntiles;
+    if (ncl > c->nclusters_cap) return AMICA_ERR_UNSUPPORTED;
+    if (c->graph) {
+        CK(cudaStreamSynchronize(c->st));
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
+    c->tc_shape = (int)shape;
+    c->S = S;
+    c->ntiles = ntiles;
+    c->nclusters = ncl;
+    c->nslots = ncl * tc_partial_groups(c->n, c->tc_shape);
+    c->hc.psi_step = tc_psi_step(c->tc_shape);
     return AMICA_OK;
 }
 
@@ -862,7 +903,7 @@ int amica_loglik_adjoint(amica_ctx* c, double* ll, double* dW, double* dmu, doub
         PartLayout PL{n, m};
         CK(cudaMemsetAsync(c->b.partial, 0, sizeof(double) * (size_t)nsl * M * PL.stride(), c->st));
     }
-    CK(launch_adjoint(a, c->NP, c->b.partial, ncl, c->st, c->use_tc));
+    CK(launch_adjoint(a, c->NP, c->b.partial, ncl, c->st, c->use_tc, c->tc_shape));
     CK(launch_adjoint_finalize(c->b.partial, c->b.raw, nsl, n, m, M, c->b.A, c->b.c,
                                c->b.beta, c->b.rho, c->d_grad, c->hc.psi_is_phi, c->st));
     TRY(check_device_error(c));
@@ -1113,12 +1154,12 @@ int amica_time_estep(amica_ctx* c, int64_t reps, double* ms_per_launch, int64_t*
     // one untimed launch, then reps timed back-to-back launches of the fused kernel
     // (the split form: its whole E-step, GEMMs included)
     if (c->use_split) TRY(enqueue_split_estep(c, a));
-    else if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st, c->hc.phi_split));
+    else if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st, c->hc.phi_split, c->tc_shape));
     else CK(launch_estep_plain(a, c->NP, c->nclusters, c->st));
     CK(cudaEventRecord(c->ev0, c->st));
     for (int64_t r = 0; r < reps; r++) {
         if (c->use_split) TRY(enqueue_split_estep(c, a));
-        else if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st, c->hc.phi_split));
+        else if (c->use_tc) CK(launch_estep_tc(a, c->NP, c->nclusters, c->st, c->hc.phi_split, c->tc_shape));
         else CK(launch_estep_plain(a, c->NP, c->nclusters, c->st));
     }
     CK(cudaEventRecord(c->ev1, c->st));
@@ -1150,7 +1191,8 @@ int amica_cohort_create(amica_ctx* const* ctxs, int64_t nsub, amica_cohort** out
     for (int64_t s = 0; s < nsub; s++) {
         const amica_ctx* c = ctxs[s];
         if (!c || c->dev != c0->dev || c->m != c0->m) return AMICA_ERR_INVALIDPARAM;
-        if (!c->use_tc || c->M != 1) return AMICA_ERR_UNSUPPORTED;
+        // the cohort kernel runs the default tile shape
+        if (!c->use_tc || c->M != 1 || c->tc_shape != 0) return AMICA_ERR_UNSUPPORTED;
     }
     CK(cudaSetDevice(c0->dev));
     amica_cohort* co = new amica_cohort();
@@ -1193,7 +1235,7 @@ int amica_cohort_create(amica_ctx* const* ctxs, int64_t nsub, amica_cohort** out
             delete co;
             return AMICA_ERR_CUDA;
         }
-        co->nslots.push_back(nitem[s] * tc_partial_groups(c->n));
+        co->nslots.push_back(nitem[s] * tc_partial_groups(c->n, 0));
     }
     co->nitems = (int)items.size();
     int r = AMICA_OK;

@@ -31,7 +31,8 @@ CFG_INT_FIELDS = (
     "nchannels", "nsamples", "nmmodels", "nsdm", "maxiter", "do_sphere", "block_size", "fix_init",
     "do_newton", "update_rho", "rho_start_iter", "newt_start_iter", "maxdec", "update_gm",
     "update_alpha", "update_A", "update_mu", "update_beta", "do_reparm", "do_reject", "rejstart",
-    "rejint", "maxrej", "precision", "device", "seed", "verbose", "max_clusters", "phi_split")
+    "rejint", "maxrej", "precision", "device", "seed", "verbose", "max_clusters", "phi_split",
+    "tc_shape")
 CFG_DBL_FIELDS = ("lrate0", "lratemax", "lnatrate", "lratefact", "rho0", "rholrate", "rhomin",
                   "rhomax", "rejsig", "phi_split_rel")
 
@@ -46,7 +47,7 @@ EXPORTED = (
     "amica_run_async", "amica_run_wait", "amica_set_grid", "amica_cohort_create",
     "amica_cohort_run", "amica_cohort_destroy", "amica_test_arm_wait_fault",
     "amica_shard_estep", "amica_shard_mstep", "amica_shard_colsum", "amica_shard_scatter",
-    "amica_shard_sphere", "amica_get_stream")
+    "amica_shard_sphere", "amica_get_stream", "amica_set_tile_shape")
 
 
 class Cfg(C.Structure):
@@ -100,6 +101,7 @@ def lib():
         L.amica_shard_mstep.argtypes = [vp, vp, _i64, C.POINTER(IterOut)]
         L.amica_shard_colsum.argtypes = [vp, vp]
         L.amica_get_stream.argtypes = [vp, C.POINTER(vp)]
+        L.amica_set_tile_shape.argtypes = [vp, _i64]
         L.amica_shard_scatter.argtypes = [vp, vp, _i64, vp]
         L.amica_shard_sphere.argtypes = [vp, vp, _i64]
         L.amica_run_wait.argtypes = [vp, C.POINTER(IterOut)]
@@ -289,6 +291,10 @@ class Amica:
         """Test hook: the next preprocess() has one missed grid-barrier arrival
         and waits bounded by wait_cycles (amica_test_arm_wait_fault)."""
         _chk(lib().amica_test_arm_wait_fault(self._ctx, int(wait_cycles)), "amica_test_arm_wait_fault")
+
+    def set_tile_shape(self, shape: int) -> None:
+        """The fused E-step's tile shape (amica_set_tile_shape): 0, 1 or 2."""
+        _chk(lib().amica_set_tile_shape(self._ctx, int(shape)), "amica_set_tile_shape")
 
     def set_grid(self, max_clusters: int) -> int:
         """Cap the E-step grid at max_clusters clusters (0: all that fit); returns

@@ -65,6 +65,11 @@ typedef struct amica_cfg {
                                both operands: 0 never, 1 always, 2 (default) from the
                                iteration after a Newton step changed every model's A by
                                less than phi_split_rel (relative, Frobenius) (new key) */
+    int64_t tc_shape;       /* mixed form up to 128 channels: tile shape of the fused E-step,
+                               0 (default) 3 density warpgroups and 48-sample tiles with 2 x
+                               stages, 1 2 warpgroups and 32-sample tiles with 2 stages, 2 the
+                               same with 3 stages (cudamica_b200.autotune picks one by
+                               measurement) (new key) */
     double lrate0, lratemax, lnatrate, lratefact, rho0, rholrate, rhomin, rhomax, rejsig;
     double phi_split_rel;   /* the threshold of phi_split = 2 (default 1e-4) (new key) */
 } amica_cfg;
@@ -243,6 +248,12 @@ int amica_shard_colsum(amica_ctx *ctx, double *d_sums);
 int amica_shard_scatter(amica_ctx *ctx, const double *d_sums_total, int64_t T_total,
                         double *d_scatter);
 int amica_shard_sphere(amica_ctx *ctx, const double *d_scatter_total, int64_t T_total);
+
+/* Switch the fused E-step's tile shape (amica_cfg.tc_shape) of a mixed-form
+ * context of at most 128 channels; the grid goes back to as many clusters as
+ * fit (the partial sums are sized for every shape).  AMICA_ERR_UNSUPPORTED for
+ * other contexts. */
+int amica_set_tile_shape(amica_ctx *ctx, int64_t shape);
 
 /* Test hook for the failure path of the bounded device waits: arms the next
  * amica_preprocess() of this context so that one block of its cooperative

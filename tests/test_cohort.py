@@ -53,6 +53,9 @@ def test_cohort_matches_subjects_fitted_alone(precision):
         eng.preprocess()
         eng.init(*init)
         eng.set_grid(coh.grids[s])
+        if coh.tile_shapes[s] >= 0:             # the subject's tuned tile shape
+            eng.set_tile_shape(coh.tile_shapes[s])
+            eng.set_grid(coh.grids[s])
         alone = eng.run(6)
         assert [o.ll for o in alone] == [o.ll for o in outs[s]], s
         pa, pc = eng.params(), coh.engines[s].params()
@@ -96,6 +99,8 @@ def test_tuned_cohort_starts_from_the_initial_state():
         eng.load_data(x)
         eng.preprocess()
         eng.init(*init)
+        assert coh.tile_shapes[s] in (0, 1, 2)
+        eng.set_tile_shape(coh.tile_shapes[s])
         eng.set_grid(coh.grids[s])
         assert [o.ll for o in eng.run(3)] == [o.ll for o in outs[s]]
         eng.close()
