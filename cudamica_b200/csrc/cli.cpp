@@ -21,7 +21,8 @@
 // word, without the quirks: precision (mixed | fp32), do_reject (on/off),
 // rejsig, rejstart, rejint, maxrej, phi_split (split correction of phi in the
 // mixed form: 0 never, 1 always, 2 automatic) and phi_split_rel (its
-// threshold), ainitfile / cinitfile (raw float32, one n x n column-major block
+// threshold), tc_shape (tile shape of the fused E-step: 0, 1 or 2),
+// ainitfile / cinitfile (raw float32, one n x n column-major block
 // / n values per model, the last block repeated for the remaining models),
 // lrate, lratemax, lnatrate, lratefact, rho0, rholrate, rhomin, rhomax,
 // maxdec, seed.
@@ -270,7 +271,8 @@ int main(int argc, char** argv) {
     }
     struct { const char* k; int64_t* p; } ints[] = {{"rejstart", &cfg.rejstart}, {"rejint", &cfg.rejint},
                                                    {"maxrej", &cfg.maxrej}, {"maxdec", &cfg.maxdec},
-                                                   {"seed", &cfg.seed}, {"phi_split", &cfg.phi_split}};
+                                                   {"seed", &cfg.seed}, {"phi_split", &cfg.phi_split},
+                                                   {"tc_shape", &cfg.tc_shape}};
     for (auto& e : ints)
         if (ext_value(L, e.k, &v)) *e.p = atol(v.c_str());
     struct { const char* k; double* p; } reals[] = {{"rejsig", &cfg.rejsig}, {"lrate", &cfg.lrate0},
