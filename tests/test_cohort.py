@@ -12,6 +12,38 @@ import pytest
 from cudamica_b200 import autotune, synth
 
 
+class _FakeEngine:
+    """Stands in for a context: E-step time per tile shape from a table."""
+
+    def __init__(self, times, kernel="tc_tf32", n=64, T=1000, M=1, m=3):
+        self.times, self.kernel = times, kernel
+        self.n, self.T, self.M, self.m = n, T, M, m
+        self.shape, self.calls = 0, []
+
+    def set_tile_shape(self, s):
+        self.shape = s
+        self.calls.append(s)
+
+    def estep_stats(self):
+        return None
+
+    def time_estep(self, reps):
+        return self.times[self.shape], 1
+
+
+def test_tile_shape_choice_is_measured_cached_and_applied():
+    autotune._cache.clear()
+    eng = _FakeEngine({0: 1.0, 1: 0.8, 2: 0.9})
+    assert autotune.best_tile_shape(eng) == 1 and eng.shape == 1
+    # the same problem shape again: from the cache, no new timing
+    other = _FakeEngine({0: 0.1, 1: 5.0, 2: 5.0})
+    assert autotune.best_tile_shape(other) == 1 and other.shape == 1 and other.calls == [1]
+    assert eng.calls == [0, 1, 2, 0, 1]     # three timed shapes, back to 0, then the choice
+    # a context outside the fused form keeps its kernel
+    assert autotune.best_tile_shape(_FakeEngine({}, kernel="plain_fp32")) == -1
+    autotune._cache.clear()
+
+
 def test_split_budget_proportional_and_bounded():
     work = [1.0, 2.0, 4.0, 1.0]
     alloc = autotune.split_budget(work, 16)
