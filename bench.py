@@ -428,8 +428,8 @@ def cohort_arm(args):
 
 def big_arm(args):
     """The 256-channel multi-model workload (synth.config4, seed 0: n=256,
-    T=2,000,000, M=4, m=5): the split mixed form (TF32 tensor-core GEMMs around
-    the density-only E-step) against plain FP32.  Device time per
+    T=2,000,000, M=4, m=5): the split mixed form (tcgen05 TF32 contraction
+    kernels around the density-only E-step) against plain FP32.  Device time per
     graph-captured iteration (CUDA events on the engine's stream), the E-step
     alone, and the LL of both forms after --big-fit-iters iterations from the
     same start (or the error that stopped a fit)."""

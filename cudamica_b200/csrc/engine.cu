@@ -97,9 +97,10 @@ struct amica_ctx {
     int n = 0, M = 0, m = 0, NP = 0, S = 0;
     int64_t T = 0;
     bool use_tc = false;
-    // split mixed form (128 < n <= 256): TF32 GEMMs around the density-only E-step
+    // split mixed form (128 < n <= 256): tcgen05 TF32 contractions around the
+    // density-only E-step
     bool use_split = false;
-    float *d_B = nullptr, *d_G = nullptr;         // T x M x NP: b = W x and g per sample
+    float *d_B = nullptr, *d_G = nullptr;         // b = W x per sample (T x M x NP); g as the Psi operand image
     float *d_Whi = nullptr, *d_Wlo = nullptr;     // M x NP x NP TF32 split of W
     float* d_xT = nullptr;                        // x^T operand image of the Psi contraction
     int adj_nclusters = 0;                        // grid of the plain gradient kernel (split form)

@@ -173,27 +173,32 @@ __global__ void __launch_bounds__(kWxThreads, 1)
                 const uint32_t xb = sbase + WxShape::OFF_X + (uint32_t)s * WxShape::X_BYTES;
                 const uint32_t dhi = tmem + kWxDhi + (uint32_t)(d * kWxN);
                 const uint32_t dlo = tmem + kWxDlo + (uint32_t)(d * kWxN);
+                // descriptors of this chunk's first K step; the others differ by
+                // constant address offsets (the address field is addr >> 4)
+                const uint64_t ad0 =
+                    sdesc(sbase + WxShape::OFF_W + (uint32_t)(kc * (kWxKC / 32) * 128 * 128), 16, 1024);
+                const uint64_t bd0 = sdesc(xb, 16, 1024);
 #pragma unroll
                 for (int kk = 0; kk < kWxKC / 8; kk++) {
                     const uint32_t koff = (uint32_t)((kk & 3) * 32);
-                    const int cbw = kc * (kWxKC / 32) + (kk >> 2);      // W_hi column block
-                    const uint64_t ad = sdesc(sbase + WxShape::OFF_W + (uint32_t)(cbw * 128 * 128) + koff, 16, 1024);
-                    const uint64_t bd = sdesc(xb + (uint32_t)((kk >> 2) * kWxN * 128) + koff, 16, 1024);
+                    const uint64_t ad = ad0 + (((uint32_t)((kk >> 2) * 128 * 128) + koff) >> 4);
+                    const uint64_t bd = bd0 + (((uint32_t)((kk >> 2) * kWxN * 128) + koff) >> 4);
                     const uint32_t acc = (kc > 0 || kk > 0) ? 1u : 0u;
                     tc_mma_tf32(dhi, ad, bd, ID, acc);
                     tc_mma_tf32_ta(dlo, tmem + (uint32_t)(kc * kWxKC + kk * 8), bd, ID, acc);
                 }
                 tc_commit(&bar[WX_EMPTY0 + s]);
                 if (kc == kWxChunks - 1) tc_commit(&bar[WX_DFULL0 + d]);
-                // the stage of the previous chunk is refilled once its MMAs have
-                // read it (they have usually finished while this chunk's were issued)
-                if (u >= 1 && u - 1 + kWxStages < nu) {
-                    const int sp = (u - 1) % kWxStages;
-                    ok = mbar_wait(&bar[WX_EMPTY0 + sp], (uint32_t)(((u - 1) / kWxStages) & 1), abort_flag,
+                // the stage of the chunk before the previous one is refilled: its
+                // MMAs have finished by now, so issuing does not wait on the
+                // tensor pipe while it still has this chunk's work queued
+                if (u >= 2 && u - 2 + kWxStages < nu) {
+                    const int sp = (u - 2) % kWxStages;
+                    ok = mbar_wait(&bar[WX_EMPTY0 + sp], (uint32_t)(((u - 2) / kWxStages) & 1), abort_flag,
                                    a.err);
                     if (!ok) break;
-                    issue(u - 1 + kWxStages);
-                    issued = u + kWxStages;
+                    issue(u - 2 + kWxStages);
+                    issued = u - 1 + kWxStages;
                 }
             }
             // drain: every load issued has landed and every MMA has completed
