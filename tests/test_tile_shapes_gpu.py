@@ -106,3 +106,30 @@ def test_autotuner_picks_a_measured_shape_and_keeps_it():
     with pytest.raises(Exception):
         plain.set_tile_shape(1)
     plain.close()
+
+
+def test_adjoint_in_every_tile_shape():
+    """The gradient sweep runs the fused kernel in the context's tile shape:
+    in every shape LL and gradients match float64 autograd of the likelihood on
+    the data as the form stores it, within the mixed form's bands (dW and dmu
+    are differences of nearly cancelling sums, so the shapes' different FP32
+    summation orders move them by a few 1e-4 of their largest entries)."""
+    import torch
+    from cudamica_b200.engine import Amica
+    from test_adjoint_config2_gpu import _as_stored as stored_adj, _rel, _torch_ref
+    n, T, M, m = 64, 60_000, 2, 3
+    xs, means, S, ldetS, A0, c0 = _data(n, T, M, m, seed=5)
+    dev = torch.device("cuda:0")
+    for shape in (0, 1, 2):
+        eng = Amica(n, T, M, m, precision=1, tc_shape=shape, update_rho=1)
+        eng.set_sphered(xs, means, S, ldetS)
+        eng.init(A0, c0)
+        eng.run(2)
+        ll_g, g_g = eng.adjoint()
+        ll_t, g_t, _, _ = _torch_ref(eng, stored_adj(xs, 1), ldetS, dev)
+        errs = {k: _rel(g_g[k], g_t[k]) for k in ("W", "mu", "beta", "rho")}
+        print(f"shape {shape}: dLL {abs(ll_g - ll_t):.2e} " + " ".join(f"{k}={v:.2e}" for k, v in errs.items()))
+        assert abs(ll_g - ll_t) < 2e-6
+        for k, v in errs.items():
+            assert v < 5e-4, (shape, k, v)
+        eng.close()
