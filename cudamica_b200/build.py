@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 SOURCES = ["engine.cu", "mstep.cu", "estep_plain.cu", "estep_tc.cu", "estep_tc_wg2.cu", "gemm_tc.cu",
-           "preprocess.cu", "adjoint.cu", "estep_noalloc.cu"]
+           "preprocess.cu", "adjoint.cu", "estep_noalloc.cu", "estep_dens.cu"]
 
 
 def _compile(src: str, verbose: bool) -> str:

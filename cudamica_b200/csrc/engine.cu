@@ -34,8 +34,8 @@ int plain_max_clusters(int n, int m, int M);
 int plain_tile_samples();
 cudaError_t launch_estep_plain(const EStepArgs& a, int NP, int nclusters, cudaStream_t st);
 bool plain_ext_supported(int n);
-int plain_ext_max_clusters(int m, int M);
-cudaError_t launch_estep_plain_ext(const EStepArgs& a, int nclusters, cudaStream_t st);
+int dens_max_clusters(int m, int M);
+cudaError_t launch_estep_dens(const EStepArgs& a, int nclusters, cudaStream_t st);
 cudaError_t launch_split_w(const float* Wf, float* whi, float* wlo, int64_t len, cudaStream_t st);
 // gemm_tc.cu
 cudaError_t launch_wx_tc(const float* x, int64_t T, const float* Whi, const float* Wlo, float* B, int M,
@@ -239,7 +239,7 @@ int enqueue_split_estep(amica_ctx* c, const EStepArgs& a) {
     const int M = c->M, NP = c->NP;
     CK(launch_split_w(c->b.Wf, c->d_Whi, c->d_Wlo, (int64_t)M * NP * NP, c->st));
     CK(launch_wx_tc(c->d_x, c->T, c->d_Whi, c->d_Wlo, c->d_B, M, c->b.err, c->st));
-    CK(launch_estep_plain_ext(a, c->nclusters, c->st));
+    CK(launch_estep_dens(a, c->nclusters, c->st));
     CK(launch_gx_tc(c->d_G, c->d_xT, c->T, c->n, c->m, M, c->b.partial, c->nslots, c->b.err, c->st));
     return AMICA_OK;
 }
@@ -414,7 +414,7 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     c->S = c->use_tc ? tc_tile_samples((int)n, c->tc_shape) : plain_tile_samples();
     c->ntiles = (int)((T + c->S - 1) / c->S);
     int maxcl = c->use_tc      ? tc_max_clusters((int)n, (int)m, (int)M, c->tc_shape)
-                : c->use_split ? plain_ext_max_clusters((int)m, (int)M)
+                : c->use_split ? dens_max_clusters((int)m, (int)M)
                                : plain_max_clusters((int)n, (int)m, (int)M);
     if (maxcl <= 0) { amica_destroy(c); return AMICA_ERR_UNSUPPORTED; }
     // partial-sum slots are sized for the full grid (and, in the fused form,
@@ -746,7 +746,7 @@ int amica_set_grid(amica_ctx* c, int64_t max_clusters, int64_t* nclusters) {
     if (c->pending >= 0) return AMICA_ERR_STATE;
     CK(cudaSetDevice(c->dev));
     int maxcl = c->use_tc      ? tc_max_clusters(c->n, c->m, c->M, c->tc_shape)
-                : c->use_split ? plain_ext_max_clusters(c->m, c->M)
+                : c->use_split ? dens_max_clusters(c->m, c->M)
                                : plain_max_clusters(c->n, c->m, c->M);
     if (maxcl <= 0) return AMICA_ERR_UNSUPPORTED;
     if (max_clusters > 0 && max_clusters < maxcl) maxcl = (int)max_clusters;

@@ -15,12 +15,6 @@
 //      src/amica.cu:1535-1550, with phi formed from Psi in the FP64 M-step).
 // Partial sums go to a per-CTA slot of `partial`; a separate kernel reduces
 // the slots in a fixed order, so results are deterministic.
-//
-// Density-only form (EXT): the two contractions run outside the kernel as
-// TF32 tensor-core GEMMs (b = W x before it, Psi = sum g x^T after it), and
-// the kernel reads its b tile from that GEMM's output and writes g per
-// sample.  One CTA then holds all NP channels of its model, so a cluster is
-// the M models of a tile stream.
 #include <cooperative_groups.h>
 #include <cstdio>
 
@@ -28,7 +22,6 @@
 
 #include "common.cuh"
 #include "density.cuh"
-#include "tc_ptx.cuh"
 
 namespace cg = cooperative_groups;
 using namespace amica;
@@ -42,9 +35,9 @@ constexpr int kS = 64;  // samples per tile
 // model holds them all; at 256 the Q = 4 CTAs of a model each own NPL = 64
 // channels (their rows of W, their densities, their rows of Psi) and read the
 // full x tile; their per-sample channel sums are added in the cluster.
-template <int NP, bool EXT = false>
+template <int NP>
 struct PlainShape {
-    static constexpr int NPL = (EXT || NP <= 128) ? NP : 64; // channels of this CTA
+    static constexpr int NPL = NP <= 128 ? NP : 64; // channels of this CTA
     static constexpr int Q = NP / NPL;              // CTAs per model
     static constexpr int SPLIT = kThreads / NPL;    // sample groups per channel
     static constexpr int SUB = kS / SPLIT;          // samples per thread per tile
@@ -54,27 +47,26 @@ struct PlainShape {
     static constexpr int NTI = NPL / 4;
     static constexpr int NTT = kThreads / NTI;
     static constexpr int CT = kS / NTT;
-    static_assert(EXT || NTI * NTT == kThreads && NTT * CT == kS, "b = W x tiling");
+    static_assert(NTI * NTT == kThreads && NTT * CT == kS, "b = W x tiling");
     // Psi update: each thread RI x RK block
     static constexpr int RI = NPL / 16;
     static constexpr int RK = NP / 16;
     static constexpr int LLD = NPL + 1;             // padded row of the lse tile
     static constexpr size_t smem_floats =
-        EXT ? (size_t)kS * NPL + (size_t)kS * LLD + 2 * kS + 2 * kS
-            : (size_t)NP * WLD + (size_t)kS * XLD + (size_t)kS * NPL + (size_t)kS * LLD +
+        (size_t)NP * WLD + (size_t)kS * XLD + (size_t)kS * NPL + (size_t)kS * LLD +
                   (size_t)kS * LLD + 2 * kS + 2 * kS;
 };
 
-template <int NP, int MM, bool EXT>
+template <int NP, int MM>
 __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
-    using Sh = PlainShape<NP, EXT>;
+    using Sh = PlainShape<NP>;
     constexpr int NPL = Sh::NPL, Q = Sh::Q;
     extern __shared__ __align__(16) float sm[];
     float* Wt = sm;                                   // [NP][WLD]  Wt[k][i] = W[i0 + i][k]
-    float* xs = EXT ? sm : Wt + NP * Sh::WLD;         // [S][XLD]
-    float* bs = EXT ? sm : xs + kS * Sh::XLD;         // [S][NPL]   (W x)_i per sample
+    float* xs = Wt + NP * Sh::WLD;                   // [S][XLD]
+    float* bs = xs + kS * Sh::XLD;                   // [S][NPL]   (W x)_i per sample
     float* gs = bs + kS * NPL;                        // [S][NPL] g; its region is [S][LLD]
-    float* lse = EXT ? gs : gs + kS * Sh::LLD;        // [S][LLD]   log-sum-exp over mixtures
+    float* lse = gs + kS * Sh::LLD;                 // [S][LLD]   log-sum-exp over mixtures
     float* slot = lse + kS * Sh::LLD;                 // [2][S]     cluster-visible L_h(t)
     float* vS = slot + 2 * kS;                        // [S]        v_h(t) (0 if not used)
 
@@ -90,7 +82,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     }
 
     // ---- resident per-CTA data: W_h^T and this thread's mixture constants
-    if constexpr (!EXT) {
+    {
         const float* Wh = a.Wf + ((size_t)h * NP + i0c) * NP;
         for (int e = tid; e < NPL * NP; e += kThreads) {
             int i = e / NP, k = e % NP;
@@ -137,7 +129,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
         for (int j = 0; j < MM; j++) dA[k][j] = 0.0;
     double dCn = 0.0, dS2 = 0.0, dGs = 0.0;
     double dLL = 0.0, dVs = 0.0;   // per-sample threads (tid < S)
-    constexpr int PRI = EXT ? 1 : Sh::RI, PRK = EXT ? 1 : Sh::RK;
+    constexpr int PRI = Sh::RI, PRK = Sh::RK;
     float psi[PRI][PRK];
 #pragma unroll
     for (int r = 0; r < PRI; r++)
@@ -147,16 +139,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     int par = 0;
     for (int tile = cid; tile < a.ntiles; tile += a.nclusters, par ^= 1) {
         const int64_t t0 = (int64_t)tile * kS;
-        if constexpr (EXT) {
-            // ---- the b tile of this model from the GEMM output (samples past T are zero)
-            const float* bsrc = a.bext + (size_t)h * NP + i0c;
-            for (int e = tid; e < kS * (NPL / 4); e += kThreads) {
-                const int t = e / (NPL / 4), i4 = e % (NPL / 4);
-                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (t0 + t < a.T) v = reinterpret_cast<const float4*>(bsrc + (t0 + t) * a.ldb)[i4];
-                *reinterpret_cast<float4*>(bs + t * NPL + 4 * i4) = v;
-            }
-        } else {
+        {
         // ---- stage the x tile (float4, coalesced; rows past T are zero)
         for (int e = tid; e < kS * (NP / 4); e += kThreads) {
             int t = e / (NP / 4), k4 = e % (NP / 4);
@@ -299,28 +282,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
                 fGs += ch_ok ? g : 0.f;
                 return g;
             };
-            if constexpr (EXT) {
-                // g of four consecutive samples per 16-byte store into the
-                // operand image of the Psi contraction (row = channel within its
-                // 128-channel half, column = sample within its 32-sample block),
-                // stored as TF32 (round to nearest, ties away) so that the MMA
-                // reads it exactly; zero past T
-                const int rr = ch & 127, hc = ch >> 7;
-#pragma unroll 1
-                for (int r4 = 0; r4 < Sh::SUB; r4 += 4) {
-                    const int64_t tg = t0 + grp * Sh::SUB + r4;
-                    float gq[4];
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        const float g = sample(grp * Sh::SUB + r4 + q);
-                        const float gt = __uint_as_float((__float_as_uint(g) + 0x1000u) & 0xffffe000u);
-                        gq[q] = (ch_ok && tg + q < a.T) ? gt : 0.f;
-                    }
-                    float* dst = a.gout + (((size_t)(tg >> 5) * a.M + h) * 2 + hc) * 4096 +
-                                 sw128_off(rr, (int)(tg & 31), 128) / 4;
-                    *reinterpret_cast<float4*>(dst) = make_float4(gq[0], gq[1], gq[2], gq[3]);
-                }
-            } else {
+            {
 #pragma unroll 2
                 for (int r = 0; r < Sh::SUB; r++) {
                     const int t = grp * Sh::SUB + r;
@@ -343,7 +305,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
         }
         __syncthreads();
         // ---- Psi_h += g x^T over the tile (thread: RI x RK block)
-        if constexpr (!EXT) {
+        {
             const int pi = tid % 16, pk = tid / 16;
             const int i0 = pi * Sh::RI, k0 = pk * Sh::RK;
 #pragma unroll 4
@@ -366,7 +328,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     PartLayout L{n, MM};
     // one slot per (cluster, channel block); entries of the other blocks stay zero
     double* out = a.partial + ((size_t)(cid * Q + cq) * M + h) * L.stride();
-    double* red = reinterpret_cast<double*>(EXT ? bs : xs);   // [SPLIT][NPL] doubles, one statistic at a time
+    double* red = reinterpret_cast<double*>(xs);   // [SPLIT][NPL] doubles, one statistic at a time
     constexpr int NACC = 7 * MM + 3;
     double vals[NACC];
 #pragma unroll
@@ -404,10 +366,7 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
         out[0] = s0;
         out[1] = s1;
     }
-    if constexpr (EXT) {
-        // Psi is summed by the GEMM after this kernel into the first slot
-        for (int e = tid; e < n * n; e += kThreads) out[L.psi() + e] = 0.0;
-    } else {
+    {
         const int pi = tid % 16, pk = tid / 16;
         const int i0 = pi * Sh::RI, k0 = pk * Sh::RK;
 #pragma unroll
@@ -422,11 +381,11 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
     cluster.sync();
 }
 
-template <int NP, int MM, bool EXT = false>
+template <int NP, int MM>
 cudaError_t launch_plain(const EStepArgs& a, int nclusters, cudaStream_t st) {
-    using Sh = PlainShape<NP, EXT>;
+    using Sh = PlainShape<NP>;
     const size_t smem = Sh::smem_floats * sizeof(float);
-    auto kern = estep_plain_kernel<NP, MM, EXT>;
+    auto kern = estep_plain_kernel<NP, MM>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     if (a.M * Sh::Q > 1) {
@@ -462,11 +421,11 @@ int plain_partial_groups(int n) { return plain_pad_channels(n) == 256 ? PlainSha
 
 // Largest cluster count whose clusters can all be resident at once (the grid
 // is persistent: every cluster loops over its share of the tiles).
-template <int NP, int MM, bool EXT = false>
+template <int NP, int MM>
 int max_active_clusters(int M) {
-    using Sh = PlainShape<NP, EXT>;
+    using Sh = PlainShape<NP>;
     const size_t smem = Sh::smem_floats * sizeof(float);
-    auto kern = estep_plain_kernel<NP, MM, EXT>;
+    auto kern = estep_plain_kernel<NP, MM>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return -1;
     const int csize = M * Sh::Q;
@@ -524,26 +483,9 @@ cudaError_t launch_estep_plain(const EStepArgs& a, int NP, int nclusters, cudaSt
     return cudaErrorInvalidValue;
 }
 
-// ---- density-only form (128 < n <= 256, mixed precision)
+// the split mixed form (128 < n <= 256) runs its density-only kernel on the
+// channels this form pads to 256
 bool plain_ext_supported(int n) { return plain_pad_channels(n) == 256; }
-
-int plain_ext_max_clusters(int m, int M) {
-    if (m < 1 || m > 5 || M < 1 || M > kMaxModels) return -1;
-#define AMICA_EXT_OCC(MMV) \
-    if (m == MMV) return max_active_clusters<256, MMV, true>(M);
-    AMICA_EXT_OCC(1) AMICA_EXT_OCC(2) AMICA_EXT_OCC(3) AMICA_EXT_OCC(4) AMICA_EXT_OCC(5)
-#undef AMICA_EXT_OCC
-    return -1;
-}
-
-cudaError_t launch_estep_plain_ext(const EStepArgs& a, int nclusters, cudaStream_t st) {
-    if (!a.bext || !a.gout || a.ldb < a.M * 256) return cudaErrorInvalidValue;
-#define AMICA_EXT_CASE(MMV) \
-    if (a.m == MMV) return launch_plain<256, MMV, true>(a, nclusters, st);
-    AMICA_EXT_CASE(1) AMICA_EXT_CASE(2) AMICA_EXT_CASE(3) AMICA_EXT_CASE(4) AMICA_EXT_CASE(5)
-#undef AMICA_EXT_CASE
-    return cudaErrorInvalidValue;
-}
 
 }  // namespace amica
 
