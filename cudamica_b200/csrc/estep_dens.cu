@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(kDT, 1) estep_dens_kernel(EStepArgs a) {
             }
         }
         // ---- phase 1: log-sum-exp over mixtures per (channel, sample), log2 units
-#pragma unroll 2
+#pragma unroll 4
         for (int r = 0; r < kDHalf; r++) {
             const int t = half * kDHalf + r;
             const float bx = (t0 + t < T) ? bst[t * kDNP + ch] : 0.f;

@@ -73,7 +73,8 @@ def compare_stats(s_gpu, s_orc, n, M, m, tight=2e-5, md_med=1e-4, md_off=1e-2, m
 
 
 @pytest.mark.parametrize("n,M,m,precision", [(256, 2, 3, 0), (200, 1, 5, 1), (160, 3, 2, 0),
-                                               (256, 4, 5, 1), (144, 2, 3, 1)])
+                                               (256, 4, 5, 1), (144, 2, 3, 1), (136, 3, 1, 1),
+                                               (192, 2, 2, 1), (176, 1, 4, 1)])
 def test_estep_stats_match_oracle(n, M, m, precision):
     T = 12000
     x, xs, means, S, ldetS, A0, c0 = case(n, T, M, m, seed=n + M)
