@@ -8,10 +8,12 @@
 // Psi contraction's operand image.
 //
 // Layout: one thread-block cluster of M CTAs (CTA h = model h) per tile
-// stream, 512 threads per CTA, one CTA per SM.  Thread (ch, half) owns
-// channel ch (0..255) and 16 of the 32 samples of a tile.  The b rows of a
-// tile arrive by bulk copies into one of two shared-memory stages; the copy of
-// the next tile is issued as the current one starts.
+// stream, 256 threads per CTA (thread = channel, all 32 samples of a tile),
+// 128 registers, two CTAs per SM: clusters of M place on any SM pair, so the
+// grid covers every SM (one 512-thread CTA per SM left 16 of 148 SMs idle at
+// M = 4), and one CTA's barrier waits are the other's issue slots.  The b rows
+// of a tile arrive by bulk copies into one of two shared-memory stages; the
+// copy of the next tile is issued as the current one starts.
 //
 // Arithmetic per element (no reciprocal): with ay = max(|y|, 2^-23),
 // L2 = log2 ay and q2 = 2^((rho - 2) L2),
@@ -20,11 +22,13 @@
 // again and the responsibility z = 2^(q - lse): 2 + 3 MUFU ops per element,
 // plus m - 1 ex2 and one lg2 per (channel, sample) for the log-sum-exp.
 //
-// Sums: FP32 per thread over kFlush tiles, then added into FP64 running sums
-// in shared memory, one per (statistic, channel), half 0 before half 1 (a
-// fixed order, so results are deterministic).  A sample whose model
-// responsibility v is exactly 0 adds exactly 0 to every sum and to g, and its
-// phase 2 is skipped (v is the same for every thread of a warp).
+// Sums: FP32 per thread over kFlush tiles, then added (red.global.add.f64)
+// into FP64 running sums that each thread owns in the Psi region of its CTA's
+// partial slot (which the Psi contraction after this kernel fills): one
+// writer per entry, so the adds land in program order and results are
+// deterministic.  A sample whose model responsibility v is exactly 0 adds
+// exactly 0 to every sum and to g, and its phase 2 is skipped (v is the same
+// for every thread of the CTA).
 #include <cooperative_groups.h>
 #include <cstdio>
 
@@ -37,18 +41,16 @@ using namespace amica;
 
 namespace {
 
-constexpr int kDT = 512;              // threads per CTA
+constexpr int kDT = 256;              // threads per CTA (one per channel); two CTAs per SM
 constexpr int kDNP = 256;             // channels (padded)
 constexpr int kDS = 32;               // samples per tile
-constexpr int kDHalf = kDS / 2;       // samples per thread per tile
 constexpr int kDLL = kDNP + 16;       // padded row of the lse tile (conflict-free reduction)
 constexpr int kFlush = 8;             // tiles between FP32 -> FP64 flushes
 
 template <int MM>
 struct DensShape {
     static constexpr int NACC = 7 * MM + 3;   // A0..A6 per mixture, sum v b, sum v b^2, sum g
-    static constexpr size_t off_acc = 0;                                        // [NACC][kDNP] double
-    static constexpr size_t off_b = off_acc + (size_t)NACC * kDNP * 8;          // [2][kDS][kDNP] float
+    static constexpr size_t off_b = 0;                                          // [2][kDS][kDNP] float
     static constexpr size_t off_lse = off_b + 2 * (size_t)kDS * kDNP * 4;       // [kDS][kDLL] float
     static constexpr size_t off_slot = off_lse + (size_t)kDS * kDLL * 4;        // [2][kDS] float
     static constexpr size_t off_v = off_slot + 2 * kDS * 4;                     // [kDS] float
@@ -173,14 +175,13 @@ __device__ __forceinline__ void issue_b_tile(const EStepArgs& a, int h, int tile
 }
 
 template <int MM>
-__global__ void __launch_bounds__(kDT, 1) estep_dens_kernel(EStepArgs a) {
+__global__ void __launch_bounds__(kDT, 2) estep_dens_kernel(EStepArgs a) {
     using Sh = DensShape<MM>;
     constexpr int NACC = Sh::NACC;
     constexpr int NPR = MM / 2;
     constexpr bool kOdd = (MM & 1) != 0;
     constexpr int NPRA = NPR > 0 ? NPR : 1;
     extern __shared__ __align__(128) unsigned char dsm[];
-    double* acc = reinterpret_cast<double*>(dsm + Sh::off_acc);   // acc[k * kDNP + ch]
     float* bs = reinterpret_cast<float*>(dsm + Sh::off_b);
     float* lse = reinterpret_cast<float*>(dsm + Sh::off_lse);
     float* slot = reinterpret_cast<float*>(dsm + Sh::off_slot);
@@ -193,16 +194,25 @@ __global__ void __launch_bounds__(kDT, 1) estep_dens_kernel(EStepArgs a) {
     const int M = a.M, n = a.n;
     const int cid = blockIdx.x / M;
     const int tid = threadIdx.x, lane = tid & 31;
-    const int ch = tid & (kDNP - 1), half = tid >> 8;
+    const int ch = tid;
     const bool ch_ok = ch < n;
     const int64_t T = a.T;
     const int ntiles = (int)((T + kDS - 1) / kDS);
-    if (a.m != MM || n > kDNP || M > kMaxModels) {   // the same in every CTA: all return
+    if (a.m != MM || n > kDNP || NACC > n || M > kMaxModels) {   // the same in every CTA: all return
         if (tid == 0) atomicOr(a.err, kErrShape);
         return;
     }
-
-    for (int e = tid; e < NACC * kDNP; e += kDT) acc[e] = 0.0;
+    // FP64 running sums: the thread of channel ch owns NACC entries (stride n)
+    // in the Psi region of the CTA's partial slot, which the Psi contraction
+    // after this kernel fills (NACC <= n).  Only the owning thread adds to an
+    // entry, so its adds land in program order and the sums are deterministic.
+    PartLayout L{n, MM};
+    double* out = a.partial + ((size_t)cid * M + h) * L.stride();
+    double* run = out + L.psi() + ch;
+    if (ch_ok) {
+#pragma unroll 1
+        for (int e = 0; e < NACC; e++) run[(size_t)e * n] = 0.0;
+    }
     if (tid == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
@@ -243,27 +253,22 @@ __global__ void __launch_bounds__(kDT, 1) estep_dens_kernel(EStepArgs a) {
         }
         fCn = 0.f; fS2 = 0.f; fGs = 0.f;
     };
-    // FP32 sums into the FP64 column of the channel (half 0, then half 1: a
-    // fixed order): entry k * MM + j is A_k of mixture j, then sum v b,
-    // sum v b^2, sum g.  Called by every thread.
+    // FP32 sums into this thread's FP64 running sums (fire-and-forget adds at
+    // L2): entry k * MM + j is A_k of mixture j, then sum v b, sum v b^2, sum g
     auto flush = [&]() {
-#pragma unroll 1
-        for (int hh = 0; hh < 2; hh++) {
-            if (half == hh) {
+        if (ch_ok) {
 #pragma unroll
-                for (int k = 0; k < 7; k++) {
+            for (int k = 0; k < 7; k++) {
 #pragma unroll
-                    for (int qq = 0; qq < NPR; qq++) {
-                        acc[(k * MM + 2 * qq) * kDNP + ch] += (double)fP[qq][k].x;
-                        acc[(k * MM + 2 * qq + 1) * kDNP + ch] += (double)fP[qq][k].y;
-                    }
-                    if constexpr (kOdd) acc[(k * MM + MM - 1) * kDNP + ch] += (double)fS1[k];
+                for (int qq = 0; qq < NPR; qq++) {
+                    red_add_f64(run + (size_t)(k * MM + 2 * qq) * n, (double)fP[qq][k].x);
+                    red_add_f64(run + (size_t)(k * MM + 2 * qq + 1) * n, (double)fP[qq][k].y);
                 }
-                acc[(7 * MM + 0) * kDNP + ch] += (double)fCn;
-                acc[(7 * MM + 1) * kDNP + ch] += (double)fS2;
-                acc[(7 * MM + 2) * kDNP + ch] += (double)fGs;
+                if constexpr (kOdd) red_add_f64(run + (size_t)(k * MM + MM - 1) * n, (double)fS1[k]);
             }
-            __syncthreads();
+            red_add_f64(run + (size_t)(7 * MM + 0) * n, (double)fCn);
+            red_add_f64(run + (size_t)(7 * MM + 1) * n, (double)fS2);
+            red_add_f64(run + (size_t)(7 * MM + 2) * n, (double)fGs);
         }
         zero_f32();
     };
@@ -292,8 +297,7 @@ __global__ void __launch_bounds__(kDT, 1) estep_dens_kernel(EStepArgs a) {
         }
         // ---- phase 1: log-sum-exp over mixtures per (channel, sample), log2 units
 #pragma unroll 4
-        for (int r = 0; r < kDHalf; r++) {
-            const int t = half * kDHalf + r;
+        for (int t = 0; t < kDS; t++) {
             const float bx = (t0 + t < T) ? bst[t * kDNP + ch] : 0.f;
             float q[MM];
 #pragma unroll
@@ -310,8 +314,9 @@ __global__ void __launch_bounds__(kDT, 1) estep_dens_kernel(EStepArgs a) {
         // j, j + 16, ... (fixed order, then a fixed butterfly), published for
         // the cluster
         float* myslot = slot + par * kDS;
-        {
-            const int t = tid >> 4, j = tid & 15;
+#pragma unroll
+        for (int t0r = 0; t0r < kDS; t0r += kDT / 16) {
+            const int t = t0r + (tid >> 4), j = tid & 15;
             float s = 0.f;
 #pragma unroll
             for (int c = 0; c < kDNP / 16; c++) s += lse[t * kDLL + c * 16 + j];
@@ -362,11 +367,11 @@ __global__ void __launch_bounds__(kDT, 1) estep_dens_kernel(EStepArgs a) {
             const int rr = ch & 127, hc = ch >> 7;
             float* gblk = a.gout + (((size_t)tile * M + h) * 2 + hc) * 4096;
 #pragma unroll 1
-            for (int r4 = 0; r4 < kDHalf; r4 += 4) {
+            for (int r4 = 0; r4 < kDS; r4 += 4) {
                 float gq[4];
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
-                    const int r = r4 + q, t = half * kDHalf + r;
+                    const int t = r4 + q;
                     const float v = vS[t];
                     float g = 0.f;
                     if (v != 0.f) {   // the same for every thread of the warp
@@ -385,7 +390,7 @@ __global__ void __launch_bounds__(kDT, 1) estep_dens_kernel(EStepArgs a) {
                     }
                     gq[q] = (ch_ok && t0 + t < T) ? tf32_rna_alu(g) : 0.f;
                 }
-                *reinterpret_cast<float4*>(gblk + sw128_off(rr, half * kDHalf + r4, 128) / 4) =
+                *reinterpret_cast<float4*>(gblk + sw128_off(rr, r4, 128) / 4) =
                     make_float4(gq[0], gq[1], gq[2], gq[3]);
             }
         }
@@ -399,12 +404,10 @@ __global__ void __launch_bounds__(kDT, 1) estep_dens_kernel(EStepArgs a) {
             if ((pend >> q) & 1u) mbar_wait(&bar[q], (pendpar >> q) & 1u, abort_flag, a.err, false, false);
     __syncthreads();
 
-    // ---- this cluster's partial sums for model h: the two halves of a channel
-    // added in a fixed order, mapped to the statistics
-    PartLayout L{n, MM};
-    double* out = a.partial + ((size_t)cid * M + h) * L.stride();
-    if (tid < kDNP && ch_ok) {
-        auto col = [&](int k) { return acc[k * kDNP + ch]; };
+    // ---- this cluster's partial sums for model h: each channel's running sums
+    // (read at L2, where the adds were made) mapped to the statistics
+    if (ch_ok) {
+        auto col = [&](int k) { return __ldcg(run + (size_t)k * n); };
 #pragma unroll 1
         for (int j = 0; j < MM; j++) {
             const float rho = a.mp[((size_t)h * MM + j) * kDNP + ch].rho;
@@ -430,6 +433,7 @@ __global__ void __launch_bounds__(kDT, 1) estep_dens_kernel(EStepArgs a) {
         out[1] = s1;
     }
     // Psi is summed by the contraction after this kernel into the first slot
+    // (the running sums in its place are read: the barrier above)
     for (int e = tid; e < n * n; e += kDT) out[L.psi() + e] = 0.0;
     // peers may still read this CTA's slots: leave together
     cluster.sync();

@@ -188,3 +188,40 @@ def test_adjoint_matches_float64_autograd_above_128_channels():
     for k in ("W", "mu", "beta", "rho"):
         assert rel_err(g_g[k], g_t[k]) < 2e-4, (k, rel_err(g_g[k], g_t[k]))
     eng.close()
+
+
+def test_split_form_per_sample_loglik_and_rejection():
+    """The split form's density kernel writes Lt per model and P per sample and
+    honours the keep mask: Lt and P per sample against the FP64 oracle on the
+    data as the form stores it (TF32), the rejection mask bit-exact against the
+    oracle's rule applied to the same P vector, and the E-step over the kept
+    samples against the oracle given the same mask."""
+    from cudamica_b200.engine import Amica
+    n, T, M, m = 160, 12000, 2, 3
+    x, xs, means, S, ldetS, A0, c0 = case(n, T, M, m, seed=5)
+    eng = Amica(n, T, M, m, precision=1, update_rho=1, rejsig=3.0)
+    assert eng.kernel == "split_tf32"
+    eng.set_sphered(xs, means, S, ldetS)
+    eng.init(A0, c0)
+    orc = O.Oracle(tf32(xs), M, m, A0, c0, ldetS, nthreads=8, update_rho=1, keep_Lt=True)
+    orc.prepare()
+    orc.estep()
+    eng.estep_stats()
+    Lt, P, keep0 = eng.loglik()
+    d = np.abs(Lt - orc.Lt) / n
+    dp = np.abs(P - orc.P) / n
+    print(f"Lt max {d.max():.2e} median {np.median(d):.2e}; P max {dp.max():.2e}")
+    assert d.max() < 4e-5 and dp.max() < 4e-5
+    Prel = eng.p_relative().astype(np.float64)
+    dropped = eng.reject_now()
+    keep1 = eng.loglik()[2]
+    k_o, d_o, _, _ = O.reject(Prel, keep0, 3.0)
+    print("rejected", dropped)
+    assert dropped == d_o and np.array_equal(keep1, k_o)
+    assert int(keep1.sum()) == T - dropped
+    orc.keep[:] = keep1
+    s_orc = orc.estep()
+    s_gpu = eng.estep_stats()
+    assert abs(s_gpu[0] - s_orc[0]) / (n * T) < 2e-6
+    compare_stats(s_gpu, s_orc, n, M, m, tight=5e-5, md_med=1e-3, md_off=0.1, md_share=0.02, phi_tol=2e-4)
+    eng.close()
