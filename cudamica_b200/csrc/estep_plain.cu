@@ -267,6 +267,9 @@ __global__ void __launch_bounds__(kThreads, 1) estep_plain_kernel(EStepArgs a) {
             // the densities, responsibilities and sums of tile sample t; returns g
             auto sample = [&](int t) -> float {
                 const float v = vS[t];
+                // a sample whose model responsibility is exactly 0 adds exactly 0
+                // to every sum and to g (v is the same in every lane of the warp)
+                if (v == 0.f) return 0.f;
                 const float bx = bs[t * NPL + ch];
                 const float nl = -lse[t * Sh::LLD + ch];
                 float2 g2 = make_float2(0.f, 0.f);
