@@ -33,7 +33,7 @@ int plain_partial_groups(int n);
 int plain_max_clusters(int n, int m, int M);
 int plain_tile_samples();
 cudaError_t launch_estep_plain(const EStepArgs& a, int NP, int nclusters, cudaStream_t st);
-bool plain_ext_supported(int n);
+bool split_form_supported(int n);
 int dens_max_clusters(int m, int M);
 cudaError_t launch_estep_dens(const EStepArgs& a, int nclusters, cudaStream_t st);
 cudaError_t launch_split_w(const float* Wf, float* whi, float* wlo, int64_t len, cudaStream_t st);
@@ -407,7 +407,7 @@ int amica_create(const amica_cfg* cfg, amica_ctx** out) {
     CK(cudaEventCreate(&c->ev1));
 
     c->use_tc = (cfg->precision == AMICA_PREC_MIXED) && tc_supported((int)n, (int)m, (int)M);
-    c->use_split = (cfg->precision == AMICA_PREC_MIXED) && !c->use_tc && plain_ext_supported((int)n) &&
+    c->use_split = (cfg->precision == AMICA_PREC_MIXED) && !c->use_tc && split_form_supported((int)n) &&
                    T <= 0x7fffffff;
     if (cfg->tc_shape < 0 || cfg->tc_shape >= tc_num_shapes()) { amica_destroy(c); return AMICA_ERR_INVALIDPARAM; }
     c->tc_shape = c->use_tc ? (int)cfg->tc_shape : 0;

@@ -488,7 +488,7 @@ cudaError_t launch_estep_plain(const EStepArgs& a, int NP, int nclusters, cudaSt
 
 // the split mixed form (128 < n <= 256) runs its density-only kernel on the
 // channels this form pads to 256
-bool plain_ext_supported(int n) { return plain_pad_channels(n) == 256; }
+bool split_form_supported(int n) { return plain_pad_channels(n) == 256; }
 
 }  // namespace amica
 
