@@ -310,9 +310,9 @@ __global__ void __launch_bounds__(kDT, 2) estep_dens_kernel(EStepArgs a) {
             lse[t * kDLL + ch] = ch_ok ? lse_mix<MM>(q) : 0.f;
         }
         __syncthreads();
-        // ---- Lt_h(t): sample t = tid / 16 summed by 16 threads over channels
-        // j, j + 16, ... (fixed order, then a fixed butterfly), published for
-        // the cluster
+        // ---- Lt_h(t): in two rounds, sample t = 16 r + tid / 16 summed by 16
+        // threads over channels j, j + 16, ... (fixed order, then a fixed
+        // butterfly), published for the cluster
         float* myslot = slot + par * kDS;
 #pragma unroll
         for (int t0r = 0; t0r < kDS; t0r += kDT / 16) {
